@@ -1,0 +1,210 @@
+"""Python front end of the decompressors: device calls on torch CUDA tensors, the host-buffer
+calls that mirror CODAG's host templates, and batched plans.
+
+Device memory and streams come from PyTorch; every decode runs in libcodag_b200.so.
+
+Mapping onto CODAG's host API (all host pointers in, a host buffer out):
+  rle_v1::decompress_gpu_orig  (include/rlev1/rlev1.h:419-592)      -> decompress_rlev1_host
+  rlev2::decompress_gpu_orig   (include/rlev2/decoder_trans.h:57-133) -> decompress_rlev2_host
+  deflate::decompress_gpu      (include/zlib/zlib.h:1583-1700)      -> decompress_deflate_host
+Unlike CODAG's templates these never print, never exit and never pick a device; errors
+raise CodagError with the per-chunk status attached.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import native
+from .native import CodagError, check
+
+_U64 = torch.int64  # torch has no uint64 for most ops; offsets are < 2^63
+
+
+def _dptr(t: torch.Tensor | None) -> int | None:
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError("expected a contiguous tensor")
+    return t.data_ptr()
+
+
+def _stream(stream: torch.cuda.Stream | None) -> int | None:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream or None
+
+
+def _status_error(where: str, status: torch.Tensor) -> None:
+    st = status.cpu().numpy()
+    bad = np.nonzero(st)[0]
+    if bad.size:
+        err = CodagError(where, int(st[bad[0]]))
+        err.chunk_status = st
+        raise err
+
+
+# --- device calls (C ABI, caller-owned device buffers) ----------------------------------------
+def decompress_rlev1(comp: torch.Tensor, blk_off: torch.Tensor, col_len: torch.Tensor, chunk_bytes: int,
+                     elem_bytes: int, out: torch.Tensor, out_bytes: int | None = None,
+                     status: torch.Tensor | None = None, stream=None) -> None:
+    """codag_decompress_rlev1: comp is the stream base (blob+8), blk_off/col_len have n entries."""
+    n = col_len.numel()
+    check("codag_decompress_rlev1", native.lib().codag_decompress_rlev1(
+        _dptr(comp), comp.numel(), _dptr(blk_off), _dptr(col_len), n, chunk_bytes, elem_bytes, _dptr(out),
+        out.numel() if out_bytes is None else out_bytes, _dptr(status), _stream(stream)))
+
+
+def decompress_rlev2(comp: torch.Tensor, blk_off: torch.Tensor, col_len: torch.Tensor, chunk_bytes: int,
+                     elem_bytes: int, out: torch.Tensor, out_bytes: int | None = None,
+                     status: torch.Tensor | None = None, stream=None) -> None:
+    """codag_decompress_rlev2: blk_off/col_len have n entries (the size entry is not passed)."""
+    n = col_len.numel()
+    check("codag_decompress_rlev2", native.lib().codag_decompress_rlev2(
+        _dptr(comp), comp.numel(), _dptr(blk_off), _dptr(col_len), n, chunk_bytes, elem_bytes, _dptr(out),
+        out.numel() if out_bytes is None else out_bytes, _dptr(status), _stream(stream)))
+
+
+def decompress_deflate(comp: torch.Tensor, blk_off: torch.Tensor, chunk_bytes: int, out: torch.Tensor,
+                       wrapper_bytes: int = 2, out_bytes: int | None = None, status: torch.Tensor | None = None,
+                       stream=None) -> None:
+    """codag_decompress_deflate: blk_off has n+1 relative offsets (blk_offset file without entry 0)."""
+    n = blk_off.numel() - 1
+    check("codag_decompress_deflate", native.lib().codag_decompress_deflate(
+        _dptr(comp), comp.numel(), _dptr(blk_off), n, chunk_bytes, wrapper_bytes, _dptr(out),
+        out.numel() if out_bytes is None else out_bytes, _dptr(status), _stream(stream)))
+
+
+def selftest_wait_timeout(wait_cycles: int = 2_000_000) -> int:
+    """Runs the bounded-wait self test and returns the status it reports (expect ETIMEOUT)."""
+    native.set_wait_limit(wait_cycles)
+    try:
+        st = torch.full((1,), -1, dtype=torch.int32, device="cuda")
+        check("codag_selftest_wait_timeout", native.lib().codag_selftest_wait_timeout(_dptr(st), _stream(None)))
+        torch.cuda.synchronize()
+        return int(st.item())
+    finally:
+        native.set_wait_limit(2_000_000_000)
+
+
+# --- host-buffer calls mirroring CODAG's templates ----------------------------------------------
+def _h2d(a: np.ndarray) -> torch.Tensor:
+    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda", non_blocking=False)
+
+
+def decompress_rlev1_host(blob: np.ndarray, blk_off: np.ndarray, col_len: np.ndarray, chunk_bytes: int = 131072,
+                          elem_bytes: int = 8) -> np.ndarray:
+    """Host blob [u64 size][streams] in, original bytes out (rle_v1::decompress_gpu_orig)."""
+    size = int(blob[:8].view(np.uint64)[0])
+    n = col_len.size
+    d_comp = _h2d(blob[8:])
+    d_off = _h2d(blk_off[:n].astype(np.uint64).view(np.int64))
+    d_len = _h2d(col_len[:n].astype(np.uint64).view(np.int64))
+    out = torch.empty(size, dtype=torch.uint8, device="cuda")
+    st = torch.zeros(n, dtype=torch.int32, device="cuda")
+    decompress_rlev1(d_comp, d_off, d_len, chunk_bytes, elem_bytes, out, size, st)
+    _status_error("rlev1", st)
+    return out.cpu().numpy()
+
+
+def decompress_rlev2_host(comp: np.ndarray, blk_off: np.ndarray, col_len: np.ndarray, chunk_bytes: int = 131072,
+                          elem_bytes: int = 8) -> np.ndarray:
+    """Host streams in, original bytes out; blk_off[n] holds the size (rlev2::decompress_gpu_orig)."""
+    n = col_len.size
+    size = int(blk_off[n])
+    d_comp = _h2d(comp)
+    d_off = _h2d(blk_off[:n].astype(np.uint64).view(np.int64))
+    d_len = _h2d(col_len.astype(np.uint64).view(np.int64))
+    out = torch.empty(size, dtype=torch.uint8, device="cuda")
+    st = torch.zeros(n, dtype=torch.int32, device="cuda")
+    decompress_rlev2(d_comp, d_off, d_len, chunk_bytes, elem_bytes, out, size, st)
+    _status_error("rlev2", st)
+    return out.cpu().numpy()
+
+
+def decompress_deflate_host(comp: np.ndarray, blk_offset: np.ndarray, chunk_bytes: int = 131072,
+                            wrapper_bytes: int = 2) -> np.ndarray:
+    """comp.bin + blk_offset.bin ([size, 0, cum...]) in, original bytes out (deflate::decompress_gpu)."""
+    size = int(blk_offset[0])
+    rel = blk_offset[1:].astype(np.uint64)
+    n = rel.size - 1
+    d_comp = _h2d(comp)
+    d_off = _h2d(rel.view(np.int64))
+    out = torch.empty(size, dtype=torch.uint8, device="cuda")
+    st = torch.zeros(n, dtype=torch.int32, device="cuda")
+    decompress_deflate(d_comp, d_off, chunk_bytes, out, wrapper_bytes, size, st)
+    _status_error("deflate", st)
+    return out.cpu().numpy()
+
+
+# --- batched persistent plans --------------------------------------------------------------------
+class BatchPlan:
+    """codag_batch_plan/run/destroy: one persistent launch over many independent chunks."""
+
+    def __init__(self, descs: np.ndarray, warps_per_cta: int | None = None, ring_slots: int | None = None,
+                 lut_bits: int | None = None):
+        descs = np.ascontiguousarray(descs, dtype=native.CHUNK_DESC_DTYPE)
+        self.n = descs.size
+        tune = None
+        if warps_per_cta is not None:
+            d = native.get_tune(native.DEFLATE)
+            tune = native.Tune(warps_per_cta, ring_slots or d.ring_slots, lut_bits or d.lut_bits, 0)
+        p = C.c_void_p()
+        check("codag_batch_plan", native.lib().codag_batch_plan(descs.ctypes.data, self.n,
+                                                                C.byref(tune) if tune is not None else None,
+                                                                C.byref(p)))
+        self._p = p
+
+    def run(self, comp: torch.Tensor, out: torch.Tensor, status: torch.Tensor | None = None, use_graph: bool = False,
+            stream=None) -> None:
+        check("codag_batch_run", native.lib().codag_batch_run(self._p, _dptr(comp), comp.numel(), _dptr(out),
+                                                              out.numel(), _dptr(status), int(use_graph),
+                                                              _stream(stream)))
+
+    def close(self) -> None:
+        if self._p:
+            native.lib().codag_batch_destroy(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class ChunkSet:
+    """Independent compressed chunks packed into one buffer, with their descriptors."""
+    comp: np.ndarray         # all streams, each starting on a 16-byte boundary
+    descs: np.ndarray        # CHUNK_DESC_DTYPE
+    out_bytes: int           # output buffer size (outputs start on 256-byte boundaries)
+
+
+def pack_chunks(streams: list[np.ndarray], codecs: list[int], elem_bytes: list[int], out_lens: list[int],
+                wrapper_bytes: int = 2) -> ChunkSet:
+    """Packs independently compressed streams into one buffer and builds their descriptors."""
+    n = len(streams)
+    descs = np.zeros(n, dtype=native.CHUNK_DESC_DTYPE)
+    comp_off = 0
+    out_off = 0
+    offs = []
+    for i, s in enumerate(streams):
+        offs.append(comp_off)
+        descs[i]["comp_off"] = comp_off
+        descs[i]["comp_len"] = s.size
+        descs[i]["out_off"] = out_off
+        descs[i]["out_len"] = out_lens[i]
+        descs[i]["codec"] = codecs[i]
+        descs[i]["elem_bytes"] = elem_bytes[i]
+        descs[i]["wrapper_bytes"] = wrapper_bytes if codecs[i] == native.DEFLATE else 0
+        comp_off += (s.size + 15) // 16 * 16
+        out_off += (out_lens[i] + 255) // 256 * 256
+    comp = np.zeros(comp_off, dtype=np.uint8)
+    for o, s in zip(offs, streams):
+        comp[o:o + s.size] = s
+    return ChunkSet(comp=comp, descs=descs, out_bytes=out_off)

@@ -1,0 +1,162 @@
+// extern "C" host entry points of the format producers: file-level layouts in CODAG's
+// on-disk format, built from the per-chunk encoders (OpenMP over chunks).
+#include <zlib.h>
+
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "host_common.hpp"
+
+using namespace codag_host;
+
+namespace {
+
+bool to_hbuf(const void* src, uint64_t bytes, codag_hbuf* dst) {
+  dst->data = static_cast<uint8_t*>(std::malloc(bytes ? bytes : 1));
+  dst->bytes = bytes;
+  if (!dst->data) return false;
+  if (bytes) std::memcpy(dst->data, src, bytes);
+  return true;
+}
+
+inline uint64_t round_up(uint64_t v, uint64_t m) { return (v + m - 1) / m * m; }
+
+bool valid_elem(int e) { return e == 1 || e == 2 || e == 4 || e == 8; }
+
+// Encodes n_chunks chunks of `padded` with `enc`; returns per-chunk streams.
+template <typename F>
+int encode_chunks(const std::vector<uint8_t>& padded, uint64_t n_chunks, uint64_t chunk_bytes,
+                  std::vector<std::vector<uint8_t>>& streams, F enc) {
+  streams.assign(n_chunks, {});
+  int failed = 0;
+#pragma omp parallel for schedule(dynamic, 8) reduction(| : failed)
+  for (int64_t i = 0; i < static_cast<int64_t>(n_chunks); i++)
+    failed |= enc(padded.data() + i * chunk_bytes, chunk_bytes, streams[i]);
+  return failed ? CODAG_EINVAL : CODAG_OK;
+}
+
+}  // namespace
+
+extern "C" void codag_hbuf_free(codag_hbuf* b) {
+  if (!b) return;
+  std::free(b->data);
+  b->data = nullptr;
+  b->bytes = 0;
+}
+
+extern "C" codag_status codag_encode_rlev1(const uint8_t* in, uint64_t in_bytes, uint64_t chunk_bytes,
+                                           int elem_bytes, codag_hbuf* blob, codag_hbuf* blk_off,
+                                           codag_hbuf* col_len) {
+  if (!in || !blob || !blk_off || !col_len || !valid_elem(elem_bytes) || chunk_bytes == 0 ||
+      chunk_bytes % elem_bytes || chunk_bytes / elem_bytes < 2 || in_bytes == 0)
+    return CODAG_EINVAL;
+  const uint64_t n = (in_bytes + chunk_bytes * 32 - 1) / (chunk_bytes * 32) * 32;  // rlev1.h:111-112
+  std::vector<uint8_t> padded(n * chunk_bytes, 0);
+  std::memcpy(padded.data(), in, in_bytes);
+  std::vector<std::vector<uint8_t>> streams;
+  if (encode_chunks(padded, n, chunk_bytes, streams, [&](const uint8_t* c, uint64_t b, std::vector<uint8_t>& o) {
+        return rlev1_encode_chunk(c, b, elem_bytes, o);
+      }))
+    return CODAG_EINVAL;
+  std::vector<uint64_t> off(n + 1, 0), len(n, 0);
+  for (uint64_t i = 0; i < n; i++) {
+    len[i] = streams[i].size();
+    off[i + 1] = off[i] + round_up(len[i], 4);  // encoder.h:780-783
+  }
+  std::vector<uint8_t> out(8 + off[n], 0);
+  std::memcpy(out.data(), &in_bytes, 8);
+  for (uint64_t i = 0; i < n; i++) std::memcpy(out.data() + 8 + off[i], streams[i].data(), len[i]);
+  if (!to_hbuf(out.data(), out.size(), blob) || !to_hbuf(off.data(), off.size() * 8, blk_off) ||
+      !to_hbuf(len.data(), len.size() * 8, col_len))
+    return CODAG_ENOMEM;
+  return CODAG_OK;
+}
+
+extern "C" codag_status codag_encode_rlev2(const uint8_t* in, uint64_t in_bytes, uint64_t chunk_bytes,
+                                           int elem_bytes, codag_hbuf* comp, codag_hbuf* blk_off,
+                                           codag_hbuf* col_len) {
+  if (!in || !comp || !blk_off || !col_len || !valid_elem(elem_bytes) || chunk_bytes == 0 ||
+      chunk_bytes % elem_bytes || in_bytes == 0)
+    return CODAG_EINVAL;
+  const uint64_t n = (in_bytes + chunk_bytes * 32 - 1) / (chunk_bytes * 32) * 32;  // encoder_trans.h:490
+  std::vector<uint8_t> padded(n * chunk_bytes, 0);
+  std::memcpy(padded.data(), in, in_bytes);
+  std::vector<std::vector<uint8_t>> streams;
+  if (encode_chunks(padded, n, chunk_bytes, streams, [&](const uint8_t* c, uint64_t b, std::vector<uint8_t>& o) {
+        return rlev2_encode_chunk(c, b, elem_bytes, o);
+      }))
+    return CODAG_EINVAL;
+  std::vector<uint64_t> off(n + 1, 0), len(n, 0);
+  for (uint64_t i = 0; i < n; i++) {
+    len[i] = streams[i].size();
+    off[i + 1] = off[i] + round_up(len[i], 128);  // encoder_trans.h:352
+  }
+  std::vector<uint8_t> out(off[n], 0);
+  for (uint64_t i = 0; i < n; i++) std::memcpy(out.data() + off[i], streams[i].data(), len[i]);
+  off[n] = in_bytes;  // encoder_trans.h:545: last entry carries the original size
+  if (!to_hbuf(out.data(), out.size(), comp) || !to_hbuf(off.data(), off.size() * 8, blk_off) ||
+      !to_hbuf(len.data(), len.size() * 8, col_len))
+    return CODAG_ENOMEM;
+  return CODAG_OK;
+}
+
+extern "C" codag_status codag_encode_deflate(const uint8_t* in, uint64_t in_bytes, uint64_t chunk_bytes,
+                                             int level, int zlib_wrapper, int require_no_stored,
+                                             codag_hbuf* comp, codag_hbuf* blk_offset, codag_hbuf* col_len) {
+  if (!in || !comp || !blk_offset || !col_len || chunk_bytes == 0 || in_bytes == 0 || level < 0 || level > 9)
+    return CODAG_EINVAL;
+  const uint64_t n = (in_bytes + chunk_bytes - 1) / chunk_bytes;  // deflate_compressor.py:62-66
+  std::vector<uint8_t> padded(n * chunk_bytes, 0);
+  std::memcpy(padded.data(), in, in_bytes);
+  std::vector<std::vector<uint8_t>> streams;
+  int stored = 0;
+  if (encode_chunks(padded, n, chunk_bytes, streams, [&](const uint8_t* c, uint64_t b, std::vector<uint8_t>& o) {
+        uint32_t types = 0;
+        int rc = deflate_encode_chunk(c, b, level, zlib_wrapper, Z_DEFAULT_STRATEGY, o, &types);
+        if (rc == CODAG_OK && (types & 0x80000001u) && require_no_stored) rc = CODAG_EINVAL;
+        o.resize(round_up(o.size(), 8), 0);  // deflate_compressor.py:104-112
+        return rc;
+      }))
+    return CODAG_EINVAL;
+  (void)stored;
+  std::vector<uint64_t> off(n + 2, 0), len(n, 0);
+  off[0] = in_bytes;
+  off[1] = 0;
+  uint64_t total = 0;
+  for (uint64_t i = 0; i < n; i++) {
+    len[i] = streams[i].size();
+    total += len[i];
+    off[i + 2] = total;
+  }
+  std::vector<uint8_t> out(total);
+  uint64_t pos = 0;
+  for (uint64_t i = 0; i < n; i++) {
+    std::memcpy(out.data() + pos, streams[i].data(), len[i]);
+    pos += len[i];
+  }
+  if (!to_hbuf(out.data(), out.size(), comp) || !to_hbuf(off.data(), off.size() * 8, blk_offset) ||
+      !to_hbuf(len.data(), len.size() * 8, col_len))
+    return CODAG_ENOMEM;
+  return CODAG_OK;
+}
+
+extern "C" codag_status codag_encode_one(int codec, const uint8_t* in, uint64_t in_bytes, int elem_bytes,
+                                         int level, codag_hbuf* stream) {
+  if (!in || !stream || in_bytes == 0) return CODAG_EINVAL;
+  std::vector<uint8_t> out;
+  int rc;
+  switch (codec) {
+    case CODAG_CODEC_RLEV1: rc = rlev1_encode_chunk(in, in_bytes, elem_bytes, out); break;
+    case CODAG_CODEC_RLEV2: rc = rlev2_encode_chunk(in, in_bytes, elem_bytes, out); break;
+    case CODAG_CODEC_DEFLATE: {
+      uint32_t types = 0;
+      rc = deflate_encode_chunk(in, in_bytes, level, 1, Z_DEFAULT_STRATEGY, out, &types);
+      if (rc == CODAG_OK && (types & 0x80000001u)) rc = CODAG_EINVAL;
+    } break;
+    default: rc = CODAG_EINVAL;
+  }
+  if (rc != CODAG_OK) return static_cast<codag_status>(rc);
+  return to_hbuf(out.data(), out.size(), stream) ? CODAG_OK : CODAG_ENOMEM;
+}

@@ -1,0 +1,535 @@
+// Kernels and extern "C" entry points of the decompressors (include/codag.h).
+//
+// Plain per-file launches: one warp per chunk, `warps_per_cta` chunks per CTA, each warp
+// with its own slice of dynamic shared memory (TMA input ring + output ring [+ Huffman
+// scratch]).  Batched launches: a persistent grid sized to the occupancy limit whose warps
+// pull chunk descriptors from a device queue (one atomic per chunk) until it is empty.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstdio>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "decode_deflate.cuh"
+#include "decode_rle.cuh"
+
+using namespace codag_dev;
+
+namespace {
+
+// ---------------------------------------------------------------------------------------
+// per-warp shared memory layouts
+// ---------------------------------------------------------------------------------------
+constexpr uint32_t align_up(uint32_t v, uint32_t a) { return (v + a - 1) / a * a; }
+
+using RleOut = OutRing<12, 10>;      // 4 KiB ring, 1 KiB drains
+using InflateOut = OutRing<13, 11>;  // 8 KiB window, 2 KiB drains
+
+template <int NSLOT>
+struct RleLayout {
+  static constexpr uint32_t kIn = 0;
+  static constexpr uint32_t kOut = kIn + NSLOT * kSlotBytes;
+  static constexpr uint32_t kBar = kOut + RleOut::kBytes;
+  static constexpr uint32_t kPerWarp = align_up(kBar + NSLOT * 8, 128);
+};
+
+template <int NSLOT, int LB>
+struct InflateLayout {
+  static constexpr uint32_t kIn = 0;
+  static constexpr uint32_t kOut = kIn + NSLOT * kSlotBytes;
+  static constexpr uint32_t kScratch = kOut + InflateOut::kBytes;
+  static constexpr uint32_t kBar = align_up(kScratch + sizeof(InflateScratch<LB>), 16);
+  static constexpr uint32_t kPerWarp = align_up(kBar + NSLOT * 8, 128);
+};
+
+struct ChunkGeom {
+  uint64_t off, len, out_base, store;
+};
+
+__device__ __forceinline__ uint64_t store_bytes(uint64_t base, uint64_t chunk_bytes, uint64_t out_bytes) {
+  return base < out_bytes ? (chunk_bytes < out_bytes - base ? chunk_bytes : out_bytes - base) : 0;
+}
+
+__device__ __forceinline__ bool stream_in_bounds(uint64_t off, uint64_t len, uint64_t comp_bytes) {
+  return off <= comp_bytes && len <= comp_bytes - off && len < (1ull << 28);
+}
+
+// ---------------------------------------------------------------------------------------
+// plain kernels: chunk = blockIdx.x * warps + warp
+// ---------------------------------------------------------------------------------------
+template <int NSLOT, int CODEC>
+__global__ void __launch_bounds__(256) k_rle_plain(const uint8_t* __restrict__ comp, uint64_t comp_bytes,
+                                                   const uint64_t* __restrict__ blk_off,
+                                                   const uint64_t* __restrict__ col_len, uint64_t n_chunks,
+                                                   uint64_t chunk_bytes, int e, uint8_t* __restrict__ out,
+                                                   uint64_t out_bytes, int32_t* __restrict__ status,
+                                                   uint64_t wait_cycles) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  using L = RleLayout<NSLOT>;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint64_t chunk = static_cast<uint64_t>(blockIdx.x) * (blockDim.x >> 5) + warp;
+  if (chunk >= n_chunks) return;
+  uint8_t* base = smem + warp * L::kPerWarp;
+  InRing<NSLOT> in;
+  in.buf = base + L::kIn;
+  in.bar = reinterpret_cast<uint64_t*>(base + L::kBar);
+  in.phase = 0;
+  in.wait_cycles = wait_cycles;
+  in.lane = lane;
+  RleOut o;
+  o.buf = base + L::kOut;
+  o.lane = lane;
+  init_ring_barriers<NSLOT>(in.bar, lane);
+
+  const uint64_t off = blk_off[chunk], len = col_len[chunk];
+  const uint64_t cbase = chunk * chunk_bytes;
+  int st;
+  if (!stream_in_bounds(off, len, comp_bytes)) {
+    st = CODAG_ECORRUPT;
+  } else {
+    in.begin(comp + off, static_cast<uint32_t>(len));
+    o.begin(out + cbase, store_bytes(cbase, chunk_bytes, out_bytes));
+    st = CODEC == CODAG_CODEC_RLEV1 ? decode_rlev1_chunk<NSLOT>(in, o, chunk_bytes, e)
+                                    : decode_rlev2_chunk<NSLOT>(in, o, chunk_bytes, e);
+  }
+  if (status && lane == 0) status[chunk] = st;
+}
+
+template <int NSLOT, int LB>
+__global__ void __launch_bounds__(256) k_inflate_plain(const uint8_t* __restrict__ comp, uint64_t comp_bytes,
+                                                       const uint64_t* __restrict__ blk_off, uint64_t n_chunks,
+                                                       uint64_t chunk_bytes, uint32_t wrapper,
+                                                       uint8_t* __restrict__ out, uint64_t out_bytes,
+                                                       int32_t* __restrict__ status, uint64_t wait_cycles) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  using L = InflateLayout<NSLOT, LB>;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint64_t chunk = static_cast<uint64_t>(blockIdx.x) * (blockDim.x >> 5) + warp;
+  if (chunk >= n_chunks) return;
+  uint8_t* base = smem + warp * L::kPerWarp;
+  InRing<NSLOT> in;
+  in.buf = base + L::kIn;
+  in.bar = reinterpret_cast<uint64_t*>(base + L::kBar);
+  in.phase = 0;
+  in.wait_cycles = wait_cycles;
+  in.lane = lane;
+  InflateOut o;
+  o.buf = base + L::kOut;
+  o.lane = lane;
+  auto& sc = *reinterpret_cast<InflateScratch<LB>*>(base + L::kScratch);
+  init_ring_barriers<NSLOT>(in.bar, lane);
+
+  const uint64_t off = blk_off[chunk], next = blk_off[chunk + 1];
+  const uint64_t cbase = chunk * chunk_bytes;
+  int st;
+  if (next < off || !stream_in_bounds(off, next - off, comp_bytes)) {
+    st = CODAG_ECORRUPT;
+  } else {
+    in.begin(comp + off, static_cast<uint32_t>(next - off));
+    o.begin(out + cbase, store_bytes(cbase, chunk_bytes, out_bytes));
+    st = decode_deflate_chunk<NSLOT, LB>(in, o, sc, chunk_bytes, wrapper);
+  }
+  if (status && lane == 0) status[chunk] = st;
+}
+
+// ---------------------------------------------------------------------------------------
+// batched persistent kernel
+// ---------------------------------------------------------------------------------------
+template <int NSLOT, int LB>
+__global__ void __launch_bounds__(256) k_batch(const codag_chunk_desc* __restrict__ descs,
+                                               const uint32_t* __restrict__ order, uint64_t n,
+                                               uint32_t* __restrict__ queue, const uint8_t* __restrict__ comp,
+                                               uint64_t comp_bytes, uint8_t* __restrict__ out, uint64_t out_bytes,
+                                               int32_t* __restrict__ status, uint64_t wait_cycles) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  using L = InflateLayout<NSLOT, LB>;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  uint8_t* base = smem + warp * L::kPerWarp;
+  InRing<NSLOT> in;
+  in.buf = base + L::kIn;
+  in.bar = reinterpret_cast<uint64_t*>(base + L::kBar);
+  in.phase = 0;
+  in.wait_cycles = wait_cycles;
+  in.lane = lane;
+  InflateOut o;
+  o.buf = base + L::kOut;
+  o.lane = lane;
+  auto& sc = *reinterpret_cast<InflateScratch<LB>*>(base + L::kScratch);
+  init_ring_barriers<NSLOT>(in.bar, lane);
+
+  for (;;) {
+    uint32_t k = 0;
+    if (lane == 0) k = atomicAdd(queue, 1u);
+    k = __shfl_sync(FULL, k, 0);
+    if (k >= n) break;
+    const uint32_t i = order[k];
+    const codag_chunk_desc d = descs[i];
+    int st;
+    const bool out_ok = d.out_off <= out_bytes && d.out_len <= out_bytes - d.out_off;
+    if (!out_ok || !stream_in_bounds(d.comp_off, d.comp_len, comp_bytes)) {
+      st = CODAG_ECORRUPT;
+    } else {
+      in.begin(comp + d.comp_off, d.comp_len);
+      o.begin(out + d.out_off, d.out_len);
+      switch (d.codec) {
+        case CODAG_CODEC_RLEV1: st = decode_rlev1_chunk<NSLOT>(in, o, d.out_len, d.elem_bytes); break;
+        case CODAG_CODEC_RLEV2: st = decode_rlev2_chunk<NSLOT>(in, o, d.out_len, d.elem_bytes); break;
+        case CODAG_CODEC_DEFLATE: st = decode_deflate_chunk<NSLOT, LB>(in, o, sc, d.out_len, d.wrapper_bytes); break;
+        default: st = CODAG_EINVAL;
+      }
+    }
+    if (status && lane == 0) status[i] = st;
+    if (st == CODAG_ETIMEOUT) break;  // ring state unknown: this warp stops pulling work
+  }
+}
+
+// A wait that no copy ever completes: exercises the bounded-wait path of InRing.
+__global__ void k_selftest_timeout(int32_t* status, uint64_t wait_cycles) {
+  __shared__ __align__(128) uint8_t buf[kSlotBytes];
+  __shared__ uint64_t bar[1];
+  const uint32_t lane = threadIdx.x & 31u;
+  InRing<1> in;
+  in.buf = buf;
+  in.bar = bar;
+  in.phase = 0;
+  in.wait_cycles = wait_cycles;
+  in.lane = lane;
+  init_ring_barriers<1>(bar, lane);
+  if (lane == 0) mbar_arrive_expect_tx(&bar[0], 16);  // 16 bytes are expected, none is sent
+  __syncwarp();
+  const bool ok = in.wait_slot(0);
+  if (lane == 0) *status = ok ? CODAG_OK : CODAG_ETIMEOUT;
+}
+
+// ---------------------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------------------
+std::mutex g_mu;
+codag_tune g_tune[3] = {{8, 4, 10, 0}, {8, 4, 10, 0}, {4, 4, 10, 0}};
+uint64_t g_wait_cycles = 2000000000ull;  // about one second at 2 GHz
+
+bool valid_slots(int s) { return s == 2 || s == 4 || s == 8; }
+bool valid_lut(int b) { return b == 9 || b == 10 || b == 11; }
+bool valid_warps(int w) { return w >= 1 && w <= 8; }
+bool valid_elem(int e) { return e == 1 || e == 2 || e == 4 || e == 8; }
+
+codag_tune tune_of(int codec) {
+  std::lock_guard<std::mutex> g(g_mu);
+  return g_tune[codec];
+}
+uint64_t wait_of() {
+  std::lock_guard<std::mutex> g(g_mu);
+  return g_wait_cycles;
+}
+
+template <class K>
+cudaError_t allow_smem(K kernel, uint32_t bytes) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+}
+
+codag_status finish_launch() {
+  const cudaError_t err = cudaGetLastError();
+  return err == cudaSuccess ? CODAG_OK : CODAG_ECUDA;
+}
+
+template <int NSLOT, int CODEC>
+codag_status launch_rle(const codag_tune& t, const uint8_t* comp, uint64_t comp_bytes, const uint64_t* blk_off,
+                        const uint64_t* col_len, uint64_t n, uint64_t chunk_bytes, int e, uint8_t* out,
+                        uint64_t out_bytes, int32_t* status, cudaStream_t s) {
+  using L = RleLayout<NSLOT>;
+  const uint32_t smem = L::kPerWarp * t.warps_per_cta;
+  auto kern = k_rle_plain<NSLOT, CODEC>;
+  if (allow_smem(kern, smem) != cudaSuccess) return CODAG_ECUDA;
+  const uint64_t grid = (n + t.warps_per_cta - 1) / t.warps_per_cta;
+  if (grid > 0x7fffffffull) return CODAG_EINVAL;
+  kern<<<static_cast<unsigned>(grid), 32 * t.warps_per_cta, smem, s>>>(comp, comp_bytes, blk_off, col_len, n,
+                                                                         chunk_bytes, e, out, out_bytes, status,
+                                                                         wait_of());
+  return finish_launch();
+}
+
+template <int NSLOT, int LB>
+codag_status launch_inflate(const codag_tune& t, const uint8_t* comp, uint64_t comp_bytes, const uint64_t* blk_off,
+                            uint64_t n, uint64_t chunk_bytes, int wrapper, uint8_t* out, uint64_t out_bytes,
+                            int32_t* status, cudaStream_t s) {
+  using L = InflateLayout<NSLOT, LB>;
+  const uint32_t smem = L::kPerWarp * t.warps_per_cta;
+  auto kern = k_inflate_plain<NSLOT, LB>;
+  if (allow_smem(kern, smem) != cudaSuccess) return CODAG_ECUDA;
+  const uint64_t grid = (n + t.warps_per_cta - 1) / t.warps_per_cta;
+  if (grid > 0x7fffffffull) return CODAG_EINVAL;
+  kern<<<static_cast<unsigned>(grid), 32 * t.warps_per_cta, smem, s>>>(comp, comp_bytes, blk_off, n, chunk_bytes,
+                                                                         static_cast<uint32_t>(wrapper), out,
+                                                                         out_bytes, status, wait_of());
+  return finish_launch();
+}
+
+template <int CODEC>
+codag_status dispatch_rle(const uint8_t* comp, uint64_t comp_bytes, const uint64_t* blk_off, const uint64_t* col_len,
+                          uint64_t n, uint64_t chunk_bytes, int e, uint8_t* out, uint64_t out_bytes, int32_t* status,
+                          cudaStream_t s) {
+  if (!comp || !blk_off || !col_len || (!out && out_bytes) || !valid_elem(e) || chunk_bytes == 0 ||
+      chunk_bytes % static_cast<uint64_t>(e))
+    return CODAG_EINVAL;
+  if (n == 0) return CODAG_OK;
+  const codag_tune t = tune_of(CODEC);
+  switch (t.ring_slots) {
+    case 2: return launch_rle<2, CODEC>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, e, out, out_bytes, status, s);
+    case 4: return launch_rle<4, CODEC>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, e, out, out_bytes, status, s);
+    default: return launch_rle<8, CODEC>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, e, out, out_bytes, status, s);
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------------------
+extern "C" codag_status codag_decompress_rlev1(const uint8_t* d_comp, uint64_t comp_bytes, const uint64_t* d_blk_off,
+                                               const uint64_t* d_col_len, uint64_t n_chunks, uint64_t chunk_bytes,
+                                               int elem_bytes, uint8_t* d_out, uint64_t out_bytes,
+                                               int32_t* d_chunk_status, codag_stream_t stream) {
+  return dispatch_rle<CODAG_CODEC_RLEV1>(d_comp, comp_bytes, d_blk_off, d_col_len, n_chunks, chunk_bytes, elem_bytes,
+                                         d_out, out_bytes, d_chunk_status, reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" codag_status codag_decompress_rlev2(const uint8_t* d_comp, uint64_t comp_bytes, const uint64_t* d_blk_off,
+                                               const uint64_t* d_col_len, uint64_t n_chunks, uint64_t chunk_bytes,
+                                               int elem_bytes, uint8_t* d_out, uint64_t out_bytes,
+                                               int32_t* d_chunk_status, codag_stream_t stream) {
+  return dispatch_rle<CODAG_CODEC_RLEV2>(d_comp, comp_bytes, d_blk_off, d_col_len, n_chunks, chunk_bytes, elem_bytes,
+                                         d_out, out_bytes, d_chunk_status, reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" codag_status codag_decompress_deflate(const uint8_t* d_comp, uint64_t comp_bytes, const uint64_t* d_blk_off,
+                                                 uint64_t n_chunks, uint64_t chunk_bytes, int wrapper_bytes,
+                                                 uint8_t* d_out, uint64_t out_bytes, int32_t* d_chunk_status,
+                                                 codag_stream_t stream) {
+  if (!d_comp || !d_blk_off || (!d_out && out_bytes) || chunk_bytes == 0 || wrapper_bytes < 0 || wrapper_bytes > 16)
+    return CODAG_EINVAL;
+  if (n_chunks == 0) return CODAG_OK;
+  const codag_tune t = tune_of(CODAG_CODEC_DEFLATE);
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+#define CODAG_INF(NS, LB) \
+  return launch_inflate<NS, LB>(t, d_comp, comp_bytes, d_blk_off, n_chunks, chunk_bytes, wrapper_bytes, d_out, out_bytes, d_chunk_status, s)
+  if (t.ring_slots == 2) {
+    if (t.lut_bits == 9) CODAG_INF(2, 9);
+    if (t.lut_bits == 10) CODAG_INF(2, 10);
+    CODAG_INF(2, 11);
+  }
+  if (t.ring_slots == 4) {
+    if (t.lut_bits == 9) CODAG_INF(4, 9);
+    if (t.lut_bits == 10) CODAG_INF(4, 10);
+    CODAG_INF(4, 11);
+  }
+  if (t.lut_bits == 9) CODAG_INF(8, 9);
+  if (t.lut_bits == 10) CODAG_INF(8, 10);
+  CODAG_INF(8, 11);
+#undef CODAG_INF
+}
+
+extern "C" codag_status codag_set_tune(int codec, const codag_tune* tune) {
+  if (codec < 0 || codec > 2 || !tune || !valid_warps(tune->warps_per_cta) || !valid_slots(tune->ring_slots) ||
+      !valid_lut(tune->lut_bits))
+    return CODAG_EINVAL;
+  std::lock_guard<std::mutex> g(g_mu);
+  g_tune[codec] = *tune;
+  return CODAG_OK;
+}
+
+extern "C" codag_status codag_get_tune(int codec, codag_tune* tune) {
+  if (codec < 0 || codec > 2 || !tune) return CODAG_EINVAL;
+  *tune = tune_of(codec);
+  return CODAG_OK;
+}
+
+extern "C" codag_status codag_set_wait_limit(uint64_t cycles) {
+  if (cycles == 0) return CODAG_EINVAL;
+  std::lock_guard<std::mutex> g(g_mu);
+  g_wait_cycles = cycles;
+  return CODAG_OK;
+}
+
+extern "C" codag_status codag_selftest_wait_timeout(int32_t* d_status, codag_stream_t stream) {
+  if (!d_status) return CODAG_EINVAL;
+  k_selftest_timeout<<<1, 32, 0, reinterpret_cast<cudaStream_t>(stream)>>>(d_status, wait_of());
+  return finish_launch();
+}
+
+// ---------------------------------------------------------------------------------------
+// batched plans
+// ---------------------------------------------------------------------------------------
+struct codag_plan {
+  uint64_t n = 0;
+  codag_tune tune{};
+  codag_chunk_desc* d_descs = nullptr;
+  uint32_t* d_order = nullptr;
+  uint32_t* d_queue = nullptr;
+  int grid = 0;
+  // captured graph and the arguments it was captured with
+  cudaGraphExec_t exec = nullptr;
+  const void* g_comp = nullptr;
+  const void* g_out = nullptr;
+  const void* g_status = nullptr;
+  uint64_t g_comp_bytes = 0, g_out_bytes = 0;
+};
+
+namespace {
+
+template <int NSLOT, int LB>
+codag_status batch_setup(codag_plan* p) {
+  using L = InflateLayout<NSLOT, LB>;
+  const uint32_t smem = L::kPerWarp * p->tune.warps_per_cta;
+  auto kern = k_batch<NSLOT, LB>;
+  if (allow_smem(kern, smem) != cudaSuccess) return CODAG_ECUDA;
+  int dev = 0, sms = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return CODAG_ECUDA;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * p->tune.warps_per_cta, smem) != cudaSuccess)
+    return CODAG_ECUDA;
+  per_sm = std::max(per_sm, 1);
+  const uint64_t need = (p->n + p->tune.warps_per_cta - 1) / p->tune.warps_per_cta;
+  p->grid = static_cast<int>(std::min<uint64_t>(need, static_cast<uint64_t>(sms) * per_sm));
+  return CODAG_OK;
+}
+
+template <int NSLOT, int LB>
+void batch_launch(codag_plan* p, const uint8_t* comp, uint64_t comp_bytes, uint8_t* out, uint64_t out_bytes,
+                  int32_t* status, cudaStream_t s) {
+  using L = InflateLayout<NSLOT, LB>;
+  const uint32_t smem = L::kPerWarp * p->tune.warps_per_cta;
+  k_batch<NSLOT, LB><<<p->grid, 32 * p->tune.warps_per_cta, smem, s>>>(p->d_descs, p->d_order, p->n, p->d_queue, comp,
+                                                                       comp_bytes, out, out_bytes, status, wait_of());
+}
+
+#define CODAG_BATCH_SWITCH(FN, ...)                      \
+  switch (p->tune.ring_slots * 100 + p->tune.lut_bits) { \
+    case 209: FN<2, 9>(__VA_ARGS__); break;              \
+    case 210: FN<2, 10>(__VA_ARGS__); break;             \
+    case 211: FN<2, 11>(__VA_ARGS__); break;             \
+    case 409: FN<4, 9>(__VA_ARGS__); break;              \
+    case 410: FN<4, 10>(__VA_ARGS__); break;             \
+    case 411: FN<4, 11>(__VA_ARGS__); break;             \
+    case 809: FN<8, 9>(__VA_ARGS__); break;              \
+    case 810: FN<8, 10>(__VA_ARGS__); break;             \
+    default: FN<8, 11>(__VA_ARGS__); break;              \
+  }
+
+codag_status batch_setup_any(codag_plan* p) {
+  codag_status st = CODAG_OK;
+  auto call = [&](auto fn) { st = fn(p); };
+  switch (p->tune.ring_slots * 100 + p->tune.lut_bits) {
+    case 209: call(batch_setup<2, 9>); break;
+    case 210: call(batch_setup<2, 10>); break;
+    case 211: call(batch_setup<2, 11>); break;
+    case 409: call(batch_setup<4, 9>); break;
+    case 410: call(batch_setup<4, 10>); break;
+    case 411: call(batch_setup<4, 11>); break;
+    case 809: call(batch_setup<8, 9>); break;
+    case 810: call(batch_setup<8, 10>); break;
+    default: call(batch_setup<8, 11>); break;
+  }
+  return st;
+}
+
+void batch_enqueue(codag_plan* p, const uint8_t* comp, uint64_t comp_bytes, uint8_t* out, uint64_t out_bytes,
+                   int32_t* status, cudaStream_t s) {
+  cudaMemsetAsync(p->d_queue, 0, sizeof(uint32_t), s);
+  CODAG_BATCH_SWITCH(batch_launch, p, comp, comp_bytes, out, out_bytes, status, s);
+}
+
+// work estimate used to order the queue: compressed bytes, Deflate weighted by its
+// per-byte decode cost relative to the RLE codecs
+uint64_t chunk_cost(const codag_chunk_desc& d) {
+  return d.codec == CODAG_CODEC_DEFLATE ? 8ull * d.comp_len + d.out_len : static_cast<uint64_t>(d.comp_len) + d.out_len / 4;
+}
+
+}  // namespace
+
+extern "C" codag_status codag_batch_plan(const codag_chunk_desc* h_descs, uint64_t n, const codag_tune* tune,
+                                         codag_plan** plan) {
+  if (!h_descs || !plan || n == 0 || n > 0xffffffffull) return CODAG_EINVAL;
+  codag_tune t = tune ? *tune : tune_of(CODAG_CODEC_DEFLATE);
+  if (!valid_warps(t.warps_per_cta) || !valid_slots(t.ring_slots) || !valid_lut(t.lut_bits)) return CODAG_EINVAL;
+  for (uint64_t i = 0; i < n; i++) {
+    const codag_chunk_desc& d = h_descs[i];
+    if (d.codec > CODAG_CODEC_DEFLATE) return CODAG_EINVAL;
+    if (d.codec != CODAG_CODEC_DEFLATE && (!valid_elem(d.elem_bytes) || d.out_len % d.elem_bytes)) return CODAG_EINVAL;
+  }
+  codag_plan* p = new (std::nothrow) codag_plan();
+  if (!p) return CODAG_ENOMEM;
+  p->n = n;
+  p->tune = t;
+  std::vector<uint32_t> order(n);
+  for (uint64_t i = 0; i < n; i++) order[i] = static_cast<uint32_t>(i);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](uint32_t a, uint32_t b) { return chunk_cost(h_descs[a]) > chunk_cost(h_descs[b]); });
+  if (cudaMalloc(&p->d_descs, n * sizeof(codag_chunk_desc)) != cudaSuccess ||
+      cudaMalloc(&p->d_order, n * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&p->d_queue, sizeof(uint32_t)) != cudaSuccess ||
+      cudaMemcpy(p->d_descs, h_descs, n * sizeof(codag_chunk_desc), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(p->d_order, order.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess) {
+    codag_batch_destroy(p);
+    return CODAG_ECUDA;
+  }
+  const codag_status st = batch_setup_any(p);
+  if (st != CODAG_OK) {
+    codag_batch_destroy(p);
+    return st;
+  }
+  *plan = p;
+  return CODAG_OK;
+}
+
+extern "C" codag_status codag_batch_run(codag_plan* p, const uint8_t* d_comp, uint64_t comp_bytes, uint8_t* d_out,
+                                        uint64_t out_bytes, int32_t* d_status, int use_graph, codag_stream_t stream) {
+  if (!p || !d_comp || !d_out) return CODAG_EINVAL;
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (!use_graph) {
+    batch_enqueue(p, d_comp, comp_bytes, d_out, out_bytes, d_status, s);
+    return finish_launch();
+  }
+  const bool same = p->exec && p->g_comp == d_comp && p->g_out == d_out && p->g_status == d_status &&
+                    p->g_comp_bytes == comp_bytes && p->g_out_bytes == out_bytes;
+  if (!same) {
+    if (p->exec) {
+      cudaGraphExecDestroy(p->exec);
+      p->exec = nullptr;
+    }
+    cudaStream_t cap;
+    if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess) return CODAG_ECUDA;
+    cudaGraph_t g = nullptr;
+    cudaError_t err = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (err == cudaSuccess) {
+      batch_enqueue(p, d_comp, comp_bytes, d_out, out_bytes, d_status, cap);
+      err = cudaStreamEndCapture(cap, &g);
+    }
+    if (err == cudaSuccess) err = cudaGraphInstantiate(&p->exec, g, 0);
+    if (g) cudaGraphDestroy(g);
+    cudaStreamDestroy(cap);
+    if (err != cudaSuccess) {
+      p->exec = nullptr;
+      cudaGetLastError();
+      return CODAG_ECUDA;
+    }
+    p->g_comp = d_comp;
+    p->g_out = d_out;
+    p->g_status = d_status;
+    p->g_comp_bytes = comp_bytes;
+    p->g_out_bytes = out_bytes;
+  }
+  return cudaGraphLaunch(p->exec, s) == cudaSuccess ? CODAG_OK : CODAG_ECUDA;
+}
+
+extern "C" codag_status codag_batch_destroy(codag_plan* p) {
+  if (!p) return CODAG_EINVAL;
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  if (p->d_descs) cudaFree(p->d_descs);
+  if (p->d_order) cudaFree(p->d_order);
+  if (p->d_queue) cudaFree(p->d_queue);
+  delete p;
+  return CODAG_OK;
+}

@@ -1,0 +1,396 @@
+// Warp decoder for one Deflate (RFC 1951) chunk.
+//
+// CODAG's decoder (include/zlib/zlib.h:807-902) decodes with 5-bit literal/length and 8-bit
+// distance lookup tables, walks code lengths 6..15 serially on a miss, copies
+// back-references with 4-byte pieces and ignores stored blocks.  This decoder keeps the
+// same one-warp-per-chunk shape but:
+//   - builds per-block lookup tables in shared memory of LB (9..11) bits for literals and
+//     lengths and 8 bits for distances, in parallel over the warp (canonical codes are
+//     tiled in MSB-first order, so each table slot finds its code by walking lengths);
+//   - keeps a 64-bit bit buffer refilled 32 bits at a time from the TMA input ring;
+//   - expands back-references warp-cooperatively out of an 8 KiB shared-memory window of
+//     the output (older sources are read back from the chunk's already-written output);
+//   - drains output in 2 KiB pieces with 16-byte vector stores;
+//   - decodes stored blocks.
+// Every lane runs the same symbol loop on the same data (shared-memory reads broadcast), so
+// control flow stays uniform and only the stores are lane-specific.
+#pragma once
+#include "device_common.cuh"
+
+namespace codag_dev {
+
+__constant__ uint16_t kLenBase[29] = {3,  4,  5,  6,  7,  8,  9,  10, 11,  13,  15,  17,  19,  23, 27,
+                                      31, 35, 43, 51, 59, 67, 83, 99, 115, 131, 163, 195, 227, 258};
+__constant__ uint8_t kLenExtra[29] = {0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 2, 2, 2,
+                                      2, 3, 3, 3, 3, 4, 4, 4, 4, 5, 5, 5, 5, 0};
+__constant__ uint16_t kDistBase[30] = {1,    2,    3,    4,    5,    7,     9,     13,    17,  25,
+                                       33,   49,   65,   97,   129,  193,   257,   385,   513, 769,
+                                       1025, 1537, 2049, 3073, 4097, 6145, 8193, 12289, 16385, 24577};
+__constant__ uint8_t kDistExtra[30] = {0, 0, 0, 0, 1, 1, 2, 2,  3,  3,  4,  4,  5,  5,  6,
+                                       6, 7, 7, 8, 8, 9, 9, 10, 10, 11, 11, 12, 12, 13, 13};
+__constant__ uint8_t kCodeLenOrder[19] = {16, 17, 18, 0, 8, 7, 9, 6, 10, 5, 11, 4, 12, 3, 13, 2, 14, 1, 15};
+
+constexpr uint32_t kDistLB = 8;
+constexpr uint32_t kCodeLenLB = 7;
+
+// table entry: [0,4) code length, [4,8) extra bits, [8,10) kind, [16,32) value
+enum : uint32_t { kKindLit = 0, kKindLen = 1, kKindEnd = 2, kKindBad = 3 };
+enum : int { kAlphaLitLen = 0, kAlphaDist = 1, kAlphaCodeLen = 2 };
+
+__device__ __forceinline__ uint32_t make_entry(uint32_t sym, uint32_t len, int alpha) {
+  if (alpha == kAlphaLitLen) {
+    if (sym < 256) return len | (kKindLit << 8) | (sym << 16);
+    if (sym == 256) return len | (kKindEnd << 8);
+    if (sym <= 285) {
+      const uint32_t k = sym - 257;
+      return len | (static_cast<uint32_t>(kLenExtra[k]) << 4) | (kKindLen << 8) | (static_cast<uint32_t>(kLenBase[k]) << 16);
+    }
+    return len | (kKindBad << 8);
+  }
+  if (alpha == kAlphaDist) {
+    if (sym < 30) return len | (static_cast<uint32_t>(kDistExtra[sym]) << 4) | (static_cast<uint32_t>(kDistBase[sym]) << 16);
+    return len | (kKindBad << 8);
+  }
+  return len | (sym << 16);
+}
+
+struct HuffTable {
+  uint32_t* lut;     // 1 << lb entries
+  uint16_t* sorted;  // symbols ordered by (code length, symbol)
+  uint32_t* cnt;     // [16] codes per length
+  uint32_t* first;   // [16] first canonical code per length
+  uint32_t* index;   // [16] position of the first code of each length in `sorted`
+  uint32_t lb;
+};
+
+// Builds `t` from code lengths lens[0..nsym).  False when the lengths over-subscribe the
+// code space.  Incomplete codes are accepted; their unused codes decode as invalid.
+__device__ bool build_table(const uint8_t* lens, uint32_t nsym, const HuffTable& t, int alpha,
+                            uint32_t* fill, uint32_t lane) {
+  if (lane < 16) t.cnt[lane] = 0;
+  __syncwarp();
+  for (uint32_t s = lane; s < nsym; s += 32) {
+    const uint32_t l = lens[s];
+    if (l) atomicAdd(&t.cnt[l], 1u);
+  }
+  __syncwarp();
+  uint32_t ok = 1;
+  if (lane == 0) {
+    uint32_t code = 0, idx = 0;
+    int left = 1;
+    for (uint32_t l = 1; l < 16; l++) {
+      t.first[l] = code;
+      code = (code + t.cnt[l]) << 1;
+      t.index[l] = idx;
+      fill[l] = idx;
+      idx += t.cnt[l];
+      left = (left << 1) - static_cast<int>(t.cnt[l]);
+      if (left < 0) ok = 0;
+    }
+  }
+  ok = __shfl_sync(FULL, ok, 0);
+  __syncwarp();
+  if (!ok) return false;
+  for (uint32_t s0 = 0; s0 < nsym; s0 += 32) {
+    const uint32_t s = s0 + lane;
+    const uint32_t l = s < nsym ? lens[s] : 0u;
+    const uint32_t grp = __match_any_sync(FULL, l);
+    const uint32_t rank = __popc(grp & lanemask_lt(lane));
+    if (l) t.sorted[fill[l] + rank] = static_cast<uint16_t>(s);
+    __syncwarp();
+    if (l && rank == 0) fill[l] += __popc(grp);
+    __syncwarp();
+  }
+  const uint32_t n = 1u << t.lb;
+  for (uint32_t x = lane; x < n; x += 32) {
+    const uint32_t v = __brev(x) >> (32 - t.lb);  // MSB-first code prefix of table slot x
+    uint32_t entry = 0;
+    for (uint32_t l = 1; l <= t.lb; l++) {
+      const uint32_t k = (v >> (t.lb - l)) - t.first[l];
+      if (k < t.cnt[l]) {
+        entry = make_entry(t.sorted[t.index[l] + k], l, alpha);
+        break;
+      }
+    }
+    t.lut[x] = entry;
+  }
+  __syncwarp();
+  return true;
+}
+
+// Codes longer than the table width: walk lengths lb+1..15 (zlib.h:459-527 does 6..15).
+__device__ __forceinline__ uint32_t slow_entry(uint64_t bb, const HuffTable& t, int alpha) {
+  const uint32_t rev = __brev(static_cast<uint32_t>(bb));
+  for (uint32_t l = t.lb + 1; l < 16; l++) {
+    const uint32_t k = (rev >> (32 - l)) - t.first[l];
+    if (k < t.cnt[l]) return make_entry(t.sorted[t.index[l] + k], l, alpha);
+  }
+  return 0;
+}
+
+// per-warp shared memory of the Deflate decoder
+template <int LB>
+struct InflateScratch {
+  uint32_t lit_lut[1u << LB];
+  uint32_t dist_lut[1u << kDistLB];
+  uint32_t lit_cnt[16], lit_first[16], lit_index[16];
+  uint32_t dist_cnt[16], dist_first[16], dist_index[16];
+  uint32_t fill[16];
+  uint16_t lit_sorted[288];
+  uint16_t dist_sorted[32];
+  uint8_t lens[320];
+};
+
+template <int NSLOT>
+struct BitReader {
+  uint64_t bb;    // pending bits, next bit in bit 0
+  uint32_t bc;    // number of pending bits
+  uint32_t wpos;  // ring position of the next 32-bit word (multiple of 4)
+
+  // append one word; returns a status (corruption = read far beyond the stream)
+  __device__ __forceinline__ int refill(InRing<NSLOT>& in) {
+    if (wpos < in.hi) {
+      const uint32_t end = min(wpos + 4, in.hi);
+      if (end > (in.waited << kSlotLog2)) {
+        // the buffer holds at most 8 bytes before wpos; everything older is consumed
+        if (!in.release(wpos >= 8 ? wpos - 8 : 0)) return CODAG_ETIMEOUT;
+        const int st = in.ensure(end);
+        if (st) return st;
+      }
+    } else if (wpos > in.hi + 16) {
+      return CODAG_ECORRUPT;
+    }
+    bb |= static_cast<uint64_t>(in.rd32(wpos)) << bc;
+    bc += 32;
+    wpos += 4;
+    return CODAG_OK;
+  }
+
+  __device__ __forceinline__ void start(InRing<NSLOT>& in, uint32_t p) {
+    wpos = p & ~3u;
+    bb = 0;
+    bc = 0;
+    (void)in;
+  }
+  __device__ __forceinline__ void drop(uint32_t n) {
+    bb >>= n;
+    bc -= n;
+  }
+  // stream position (ring coordinates) of the next unread bit, times 8
+  __device__ __forceinline__ uint64_t bitpos() const { return static_cast<uint64_t>(wpos) * 8u - bc; }
+};
+
+template <int NSLOT, int LB, class OUT>
+__device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<LB>& sc, uint64_t chunk_bytes,
+                                    uint32_t wrapper) {
+  const uint32_t lane = in.lane;
+  const uint64_t cap = chunk_bytes;
+  const HuffTable lit{sc.lit_lut, sc.lit_sorted, sc.lit_cnt, sc.lit_first, sc.lit_index, LB};
+  const HuffTable dst{sc.dist_lut, sc.dist_sorted, sc.dist_cnt, sc.dist_first, sc.dist_index, kDistLB};
+  const HuffTable cl{sc.dist_lut, sc.dist_sorted, sc.dist_cnt, sc.dist_first, sc.dist_index, kCodeLenLB};
+  constexpr uint32_t kOutMask = OUT::kMask;
+
+  uint64_t op = 0;  // bytes produced
+  int st = CODAG_OK;
+  BitReader<NSLOT> br;
+  bool fixed_ready = false;
+
+  if (in.lo + wrapper > in.hi) st = CODAG_ECORRUPT;
+  if (!st && !in.release(in.lo)) st = CODAG_ETIMEOUT;
+  const uint32_t start = in.lo + wrapper;
+  br.start(in, start);
+  if (!st) st = br.refill(in);
+  if (!st) br.drop((start & 3u) * 8u);
+
+#define CODAG_REFILL()                   \
+  if (br.bc < 32) {                      \
+    st = br.refill(in);                  \
+    if (st) break;                       \
+  }
+
+  bool last = false;
+  while (!st && !last) {
+    if (br.bitpos() > static_cast<uint64_t>(in.hi) * 8u) { st = CODAG_ECORRUPT; break; }
+    CODAG_REFILL();
+    last = br.bb & 1u;
+    const uint32_t btype = static_cast<uint32_t>(br.bb >> 1) & 3u;
+    br.drop(3);
+    if (btype == 0) {  // stored block
+      br.drop(br.bc & 7u);
+      CODAG_REFILL();
+      const uint32_t len = static_cast<uint32_t>(br.bb) & 0xffffu;
+      const uint32_t nlen = static_cast<uint32_t>(br.bb >> 16) & 0xffffu;
+      br.drop(32);
+      if (len != (~nlen & 0xffffu)) { st = CODAG_ECORRUPT; break; }
+      uint32_t p = br.wpos - br.bc / 8u;
+      if (p + len > in.hi || op + len > cap) { st = CODAG_ECORRUPT; break; }
+      uint32_t left = len;
+      while (left) {
+        const uint32_t piece = left < 1024u ? left : 1024u;
+        if (!in.release(p)) { st = CODAG_ETIMEOUT; break; }
+        st = in.ensure(p + piece);
+        if (st) break;
+        for (uint32_t t = lane; t < piece; t += 32) out.buf[(op + t) & kOutMask] = static_cast<uint8_t>(in.rd8(p + t));
+        op += piece;
+        p += piece;
+        left -= piece;
+        __syncwarp();
+        out.flush_to(op);
+      }
+      if (st) break;
+      br.start(in, p);
+      st = br.refill(in);
+      if (st) break;
+      br.drop((p & 3u) * 8u);
+      continue;
+    }
+    if (btype == 3) { st = CODAG_ECORRUPT; break; }
+    if (btype == 1) {  // fixed Huffman codes (RFC 1951 3.2.6)
+      if (!fixed_ready) {
+        for (uint32_t s = lane; s < 320; s += 32)
+          sc.lens[s] = s < 144 ? 8 : s < 256 ? 9 : s < 280 ? 7 : s < 288 ? 8 : 5;
+        __syncwarp();
+        build_table(sc.lens, 288, lit, kAlphaLitLen, sc.fill, lane);
+        build_table(sc.lens + 288, 30, dst, kAlphaDist, sc.fill, lane);
+        fixed_ready = true;
+      }
+    } else {  // dynamic Huffman codes (zlib.h:607-707)
+      fixed_ready = false;
+      CODAG_REFILL();
+      const uint32_t hlit = (static_cast<uint32_t>(br.bb) & 31u) + 257u;
+      const uint32_t hdist = (static_cast<uint32_t>(br.bb >> 5) & 31u) + 1u;
+      const uint32_t hclen = (static_cast<uint32_t>(br.bb >> 10) & 15u) + 4u;
+      br.drop(14);
+      if (hlit > 286 || hdist > 30) { st = CODAG_ECORRUPT; break; }
+      // code length code lengths, 3 bits each in kCodeLenOrder order
+      for (uint32_t i0 = 0; i0 < 19; i0 += 10) {
+        CODAG_REFILL();
+        const uint32_t i = i0 + lane;
+        if (lane < 10 && i < 19) {
+          const uint32_t v = i < hclen ? static_cast<uint32_t>(br.bb >> (3 * lane)) & 7u : 0u;
+          sc.lens[kCodeLenOrder[i]] = static_cast<uint8_t>(v);
+        }
+        const uint32_t took = hclen > i0 ? min(hclen - i0, 10u) : 0u;
+        br.drop(3 * took);
+      }
+      if (st) break;
+      __syncwarp();
+      if (!build_table(sc.lens, 19, cl, kAlphaCodeLen, sc.fill, lane)) { st = CODAG_ECORRUPT; break; }
+      // literal/length and distance code lengths, run-length coded with symbols 16..18
+      uint32_t idx = 0, prev = 0;
+      const uint32_t total = hlit + hdist;
+      while (idx < total) {
+        CODAG_REFILL();
+        const uint32_t e = cl.lut[br.bb & ((1u << kCodeLenLB) - 1u)];
+        if (!e) { st = CODAG_ECORRUPT; break; }
+        br.drop(e & 15u);
+        const uint32_t sym = e >> 16;
+        if (sym < 16) {
+          if (lane == 0) sc.lens[idx] = static_cast<uint8_t>(sym);
+          prev = sym;
+          idx++;
+          continue;
+        }
+        uint32_t rep, val = 0;
+        if (sym == 16) {
+          if (idx == 0) { st = CODAG_ECORRUPT; break; }
+          val = prev;
+          rep = 3u + (static_cast<uint32_t>(br.bb) & 3u);
+          br.drop(2);
+        } else if (sym == 17) {
+          rep = 3u + (static_cast<uint32_t>(br.bb) & 7u);
+          br.drop(3);
+        } else {
+          rep = 11u + (static_cast<uint32_t>(br.bb) & 127u);
+          br.drop(7);
+        }
+        if (idx + rep > total) { st = CODAG_ECORRUPT; break; }
+        for (uint32_t t = lane; t < rep; t += 32) sc.lens[idx + t] = static_cast<uint8_t>(val);
+        prev = val;
+        idx += rep;
+      }
+      if (st) break;
+      __syncwarp();
+      if (sc.lens[256] == 0) { st = CODAG_ECORRUPT; break; }
+      // the distance lengths follow the literal/length lengths; move them to their slot
+      uint8_t dl = 0;
+      if (lane < hdist) dl = sc.lens[hlit + lane];
+      __syncwarp();
+      for (uint32_t s = hlit + lane; s < 288; s += 32) sc.lens[s] = 0;
+      __syncwarp();
+      if (lane < 32) sc.lens[288 + lane] = lane < hdist ? dl : 0;
+      __syncwarp();
+      if (!build_table(sc.lens, hlit, lit, kAlphaLitLen, sc.fill, lane)) { st = CODAG_ECORRUPT; break; }
+      if (!build_table(sc.lens + 288, hdist, dst, kAlphaDist, sc.fill, lane)) { st = CODAG_ECORRUPT; break; }
+    }
+
+    // symbol loop (zlib.h:712-805)
+    for (;;) {
+      CODAG_REFILL();
+      uint32_t e = lit.lut[br.bb & ((1u << LB) - 1u)];
+      if (!e) {
+        e = slow_entry(br.bb, lit, kAlphaLitLen);
+        if (!e) { st = CODAG_ECORRUPT; break; }
+      }
+      const uint32_t kind = (e >> 8) & 3u;
+      br.drop(e & 15u);
+      if (kind == kKindLit) {
+        if (op >= cap) { st = CODAG_ECORRUPT; break; }
+        if (lane == 0) out.buf[op & kOutMask] = static_cast<uint8_t>(e >> 16);
+        op++;
+        if (op - out.flushed >= OUT::kFlush) out.flush_to(op);
+        continue;
+      }
+      if (kind == kKindEnd) break;
+      if (kind == kKindBad) { st = CODAG_ECORRUPT; break; }
+      const uint32_t lext = (e >> 4) & 15u;
+      const uint32_t len = (e >> 16) + (static_cast<uint32_t>(br.bb) & ((1u << lext) - 1u));
+      br.drop(lext);
+      CODAG_REFILL();
+      uint32_t d = dst.lut[br.bb & ((1u << kDistLB) - 1u)];
+      if (!d) {
+        d = slow_entry(br.bb, dst, kAlphaDist);
+        if (!d) { st = CODAG_ECORRUPT; break; }
+      }
+      if ((d >> 8) & 3u) { st = CODAG_ECORRUPT; break; }
+      br.drop(d & 15u);
+      const uint32_t dext = (d >> 4) & 15u;
+      const uint32_t dist = (d >> 16) + (static_cast<uint32_t>(br.bb) & ((1u << dext) - 1u));
+      br.drop(dext);
+      if (dist > op || op + len > cap) { st = CODAG_ECORRUPT; break; }
+      __syncwarp();
+      if (dist + len <= OUT::kBytes) {  // source still in the shared-memory window
+        if (dist >= len) {
+          for (uint32_t t = lane; t < len; t += 32) out.buf[(op + t) & kOutMask] = out.buf[(op - dist + t) & kOutMask];
+        } else {
+          uint32_t r = lane % dist;
+          const uint32_t step = 32u % dist;
+          for (uint32_t t = lane; t < len; t += 32) {
+            out.buf[(op + t) & kOutMask] = out.buf[(op - dist + r) & kOutMask];
+            r += step;
+            if (r >= dist) r -= dist;
+          }
+        }
+      } else {  // older than the window: read back the chunk's flushed output
+        const uint64_t src0 = op - dist;
+        uint32_t r = dist >= len ? lane : lane % dist;
+        const uint32_t step = dist >= len ? 32u : 32u % dist;
+        for (uint32_t t = lane; t < len; t += 32) {
+          const uint64_t s = src0 + r;
+          out.buf[(op + t) & kOutMask] = s < out.store ? out.gdst[s] : 0;  // unstored bytes are never stored either
+          r += step;
+          if (dist < len && r >= dist) r -= dist;
+        }
+      }
+      op += len;
+      if (op - out.flushed >= OUT::kFlush) out.flush_to(op);
+    }
+  }
+#undef CODAG_REFILL
+  if (!in.drain() && st == CODAG_OK) st = CODAG_ETIMEOUT;
+  out.finish(op);
+  if (st == CODAG_OK && (op < out.store || br.bitpos() > static_cast<uint64_t>(in.hi) * 8u)) st = CODAG_ECORRUPT;
+  return st;
+}
+
+}  // namespace codag_dev

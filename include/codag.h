@@ -1,0 +1,177 @@
+/*
+ * codag.h -- C ABI of the B200-native CODAG chunk decompressors.
+ *
+ * Every pointer named d_* is a DEVICE pointer owned by the caller.  Calls are asynchronous
+ * on `stream` (a cudaStream_t; NULL = legacy default stream), allocate no device memory,
+ * never print and never exit.  The return value reports argument and launch errors only;
+ * stream corruption and bounded-wait timeouts are reported per chunk in d_chunk_status
+ * (CODAG_OK / CODAG_ECORRUPT / CODAG_ETIMEOUT), which may be NULL when not wanted.
+ * Distinct streams may be used from distinct host threads concurrently.
+ *
+ * Output contract shared by the three decoders: chunk i decodes to
+ * d_out + i*chunk_bytes; bytes beyond out_bytes are decoded but not stored, so out_bytes
+ * may be the exact original size.  A chunk is OK when its stream is well formed and the
+ * bytes it produced cover its stored part without exceeding chunk_bytes.
+ */
+#ifndef CODAG_H
+#define CODAG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *codag_stream_t; /* same type as cudaStream_t */
+
+typedef enum {
+    CODAG_OK = 0,
+    CODAG_EINVAL = 1,   /* bad argument (null pointer, size, alignment, element width) */
+    CODAG_ECORRUPT = 2, /* malformed stream (per chunk) */
+    CODAG_ETIMEOUT = 3, /* a bounded device wait ran out (per chunk) */
+    CODAG_ECUDA = 4,    /* a CUDA runtime call or launch failed */
+    CODAG_ENOMEM = 5    /* host allocation failed (planning calls only) */
+} codag_status;
+
+enum { CODAG_CODEC_RLEV1 = 0, CODAG_CODEC_RLEV2 = 1, CODAG_CODEC_DEFLATE = 2 };
+
+/*
+ * ORC RLE v1, one stream per chunk.
+ * Replaces rle_v1::decompress_gpu_orig<...> (include/rlev1/rlev1.h:419-592), which takes the
+ * host blob [u64 original_bytes][streams] and reads ./input_data/rle_v1_{col_len,blk_offset}.bin.
+ *   d_comp      stream base, i.e. blob + 8 (the kernel argument d_in+8 at rlev1.h:513)
+ *   comp_bytes  readable bytes at d_comp (every stream must lie inside)
+ *   d_blk_off   n_chunks offsets: stream i starts at d_comp + d_blk_off[i]
+ *   d_col_len   n_chunks exact stream lengths in bytes
+ *   chunk_bytes decoded bytes per chunk (131072 in CODAG), a multiple of elem_bytes
+ *   elem_bytes  1, 2, 4 or 8 (the DATA_TYPE template argument)
+ */
+codag_status codag_decompress_rlev1(const uint8_t *d_comp, uint64_t comp_bytes,
+                                    const uint64_t *d_blk_off, const uint64_t *d_col_len,
+                                    uint64_t n_chunks, uint64_t chunk_bytes, int elem_bytes,
+                                    uint8_t *d_out, uint64_t out_bytes, int32_t *d_chunk_status,
+                                    codag_stream_t stream);
+
+/*
+ * ORC RLE v2 (unsigned variant), one stream per chunk.
+ * Replaces rlev2::decompress_gpu_orig<...> (include/rlev2/decoder_trans.h:57-133), whose
+ * arguments (in, n_chunks, blk_off, col_len, CHUNK_SIZE) map one to one onto these.
+ *   d_blk_off   n_chunks offsets (128-byte aligned in CODAG's layout)
+ *   d_col_len   n_chunks exact stream lengths
+ */
+codag_status codag_decompress_rlev2(const uint8_t *d_comp, uint64_t comp_bytes,
+                                    const uint64_t *d_blk_off, const uint64_t *d_col_len,
+                                    uint64_t n_chunks, uint64_t chunk_bytes, int elem_bytes,
+                                    uint8_t *d_out, uint64_t out_bytes, int32_t *d_chunk_status,
+                                    codag_stream_t stream);
+
+/*
+ * Deflate, one stream per chunk.
+ * Replaces deflate::decompress_gpu<...> (include/zlib/zlib.h:1583-1700), which reads the
+ * <name>_blk_offset.bin array [original_bytes, 0, cum_1 .. cum_n] and passes blk_offset+1.
+ *   d_blk_off     n_chunks+1 relative offsets (the array above without its first entry);
+ *                 stream i is d_comp[d_blk_off[i] .. d_blk_off[i+1])
+ *   wrapper_bytes header bytes skipped before the Deflate data: 2 for zlib-wrapped streams
+ *                 (what CODAG's decoder assumes, zlib.h:819), 0 for raw Deflate
+ * Stored blocks are decoded (CODAG's decoder ignores them, zlib.h:840-842).
+ */
+codag_status codag_decompress_deflate(const uint8_t *d_comp, uint64_t comp_bytes,
+                                      const uint64_t *d_blk_off, uint64_t n_chunks,
+                                      uint64_t chunk_bytes, int wrapper_bytes, uint8_t *d_out,
+                                      uint64_t out_bytes, int32_t *d_chunk_status,
+                                      codag_stream_t stream);
+
+/* --- launch tuning --------------------------------------------------------------------
+ * Process-wide launch shape for the per-file calls above, per codec.  warps_per_cta is
+ * the number of chunks one CTA decodes (one warp per chunk); ring_slots the depth of the
+ * TMA input ring (2, 4 or 8 slots of 1 KiB); lut_bits the primary Huffman table width
+ * (Deflate only: 9, 10 or 11).  Values outside the supported sets return CODAG_EINVAL. */
+typedef struct {
+    int32_t warps_per_cta;
+    int32_t ring_slots;
+    int32_t lut_bits;
+    int32_t reserved;
+} codag_tune;
+
+codag_status codag_set_tune(int codec, const codag_tune *tune);
+codag_status codag_get_tune(int codec, codag_tune *tune);
+
+/* Upper bound, in GPU clock cycles, of every device-side wait (default about one second).
+ * A wait that runs out marks its chunk CODAG_ETIMEOUT and the warp stops cleanly. */
+codag_status codag_set_wait_limit(uint64_t cycles);
+
+/* Launch a kernel whose only warp waits on a TMA barrier that no copy ever completes,
+ * bounded by the wait limit, and writes the resulting status (CODAG_ETIMEOUT) to
+ * *d_status.  Used to test the timeout path without faulting or hanging a GPU. */
+codag_status codag_selftest_wait_timeout(int32_t *d_status, codag_stream_t stream);
+
+/* --- batched persistent decompression ------------------------------------------------
+ * Thousands of independently compressed chunks of uneven size and mixed codec, decoded
+ * by one persistent launch that pulls work from a device queue ordered by estimated cost
+ * (largest first).  There is no counterpart in CODAG, whose kernels assume one uniform
+ * chunk size per launch; the per-chunk decoders are the ones behind the calls above. */
+typedef struct {
+    uint64_t comp_off;     /* stream byte offset in d_comp */
+    uint64_t out_off;      /* output byte offset in d_out */
+    uint32_t comp_len;     /* stream bytes */
+    uint32_t out_len;      /* decoded bytes */
+    uint8_t codec;         /* CODAG_CODEC_* */
+    uint8_t elem_bytes;    /* RLE element width */
+    uint8_t wrapper_bytes; /* Deflate header bytes to skip */
+    uint8_t reserved[5];
+} codag_chunk_desc;
+
+typedef struct codag_plan codag_plan;
+
+/* Copies the descriptors to the device (the only allocating call), orders the queue and
+ * picks the launch shape (tune may be NULL: use the process-wide defaults). */
+codag_status codag_batch_plan(const codag_chunk_desc *h_descs, uint64_t n, const codag_tune *tune,
+                              codag_plan **plan);
+/* One persistent launch over all planned chunks; d_status has n entries (may be NULL).
+ * With use_graph != 0 the launch is captured once into a CUDA graph for these pointers
+ * and replayed on later calls with the same pointers. */
+codag_status codag_batch_run(codag_plan *plan, const uint8_t *d_comp, uint64_t comp_bytes,
+                             uint8_t *d_out, uint64_t out_bytes, int32_t *d_status, int use_graph,
+                             codag_stream_t stream);
+codag_status codag_batch_destroy(codag_plan *plan);
+
+/* --- host-side format producers (CPU; used by the CLIs, tests and benchmarks) ---------- */
+typedef struct {
+    uint8_t *data;
+    uint64_t bytes;
+} codag_hbuf; /* malloc'd by the library; release with codag_hbuf_free */
+void codag_hbuf_free(codag_hbuf *b);
+
+/* CODAG's RLE v1 layout (include/rlev1/rlev1.h:103-192): blob = [u64 in_bytes][streams],
+ * blk_off = n_pad+1 u64 (stream i at blob+8+blk_off[i], 4-byte aligned), col_len = n_pad u64,
+ * n_pad = ceil(in_bytes/(chunk*32))*32 chunks over the zero-padded input. */
+codag_status codag_encode_rlev1(const uint8_t *in, uint64_t in_bytes, uint64_t chunk_bytes,
+                                int elem_bytes, codag_hbuf *blob, codag_hbuf *blk_off,
+                                codag_hbuf *col_len);
+/* CODAG's RLE v2 layout (include/rlev2/encoder_trans.h:482-564): streams at 128-byte aligned
+ * blk_off[i]; blk_off has n_pad+1 entries with blk_off[n_pad] = in_bytes; col_len n_pad. */
+codag_status codag_encode_rlev2(const uint8_t *in, uint64_t in_bytes, uint64_t chunk_bytes,
+                                int elem_bytes, codag_hbuf *comp, codag_hbuf *blk_off,
+                                codag_hbuf *col_len);
+/* CODAG's Deflate layout (deflate_compressor.py:44-125): input zero padded to a multiple of
+ * chunk_bytes; comp = zlib streams each padded to 8 bytes; blk_offset = n+2 u64
+ * [in_bytes, 0, cum_1 .. cum_n]; col_len = n padded sizes.  zlib_wrapper=1 writes RFC 1950
+ * streams (CODAG's format), 0 raw Deflate.  Fails with CODAG_EINVAL if require_no_stored and
+ * zlib emitted a stored block. */
+codag_status codag_encode_deflate(const uint8_t *in, uint64_t in_bytes, uint64_t chunk_bytes,
+                                  int level, int zlib_wrapper, int require_no_stored,
+                                  codag_hbuf *comp, codag_hbuf *blk_offset, codag_hbuf *col_len);
+/* One stream of a single buffer (the batched workload's per-chunk files). */
+codag_status codag_encode_one(int codec, const uint8_t *in, uint64_t in_bytes, int elem_bytes,
+                              int level, codag_hbuf *stream);
+
+/* Seeded synthetic columns (splitmix64/xoshiro256**). */
+void codag_gen_rlev1_column(uint64_t n, uint64_t seed, int elem_bytes, uint8_t *out);
+void codag_gen_rlev2_column(uint64_t n, uint64_t seed, int elem_bytes, uint8_t *out);
+void codag_gen_text(uint64_t bytes, uint64_t seed, uint8_t *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CODAG_H */

@@ -1,0 +1,50 @@
+"""Regenerates the golden files of tests/golden from CODAG's own Python compressor.
+
+Runs only where the CODAG tree is available (default /root/reference, or $CODAG_REF).
+deflate_compressor.py imports `zstandard` at module level without using it on this path,
+and writes to a hard-coded directory; the script stubs the first and redirects the second
+into this folder, then calls CODAG's zlib_chunk_compress (deflate_compressor.py:44-125)
+on a seeded text sample.  The tests compare our layout writer against these files.
+
+    python tests/golden/make_golden.py
+"""
+import builtins
+import os
+import sys
+import types
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parents[1]
+REF = Path(os.environ.get("CODAG_REF", "/root/reference"))
+
+
+def main() -> None:
+    sys.path.insert(0, str(REPO))
+    from codag_b200 import native
+
+    src = native.gen_text(140_000, 424242)
+    (HERE / "deflate_src.bin").write_bytes(src.tobytes())
+
+    sys.modules.setdefault("zstandard", types.ModuleType("zstandard"))
+    sys.path.insert(0, str(REF))
+    import deflate_compressor as dc  # CODAG's compressor
+
+    prefix = "/home/jpark346/compressor/output/"
+
+    def redirected_open(path, *args, **kwargs):
+        if isinstance(path, str) and path.startswith(prefix):
+            path = str(HERE / path[len(prefix):])
+        return builtins.open(path, *args, **kwargs)
+
+    dc.open = redirected_open
+    dc.print = lambda *a, **k: None
+    dc.zlib_chunk_compress(src.tobytes(), "deflate_ref")
+    for name in ("deflate_ref_comp.bin", "deflate_ref_blk_offset.bin", "deflate_ref_col_len.bin"):
+        print(name, (HERE / name).stat().st_size)
+
+
+if __name__ == "__main__":
+    main()
