@@ -1,0 +1,350 @@
+#!/usr/bin/env python
+"""Benchmark of the chunked decompressors on one node (one process per GPU).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload rlev2|rlev1|rlev1x128|deflate|batched]
+
+Default workload (rlev2): CODAG's RLE v2 configuration -- 134,217,728 int64 values (1 GiB)
+of seeded synthetic segments in 8,192 chunks of 128 KiB, decoded by one plain per-file
+launch per step.  Inputs (compressed + decompressed, about 1.2 GB) exceed the 126 MB L2,
+so no flush is needed between steps.  N>1: every rank decodes its own instance (weak
+scaling, no collective on the data path; timing is the max over ranks).
+
+Prints one JSON line (rank 0).  `value` is decompressed GB/s with inputs resident in HBM;
+`e2e` is the same metric through the host-buffer API (pinned H2D of the streams and
+metadata, decode, D2H of the output, every step); `roofline` relates the decode kernel's
+algorithmic bytes (compressed bytes read + decompressed bytes written) to the measured
+HBM copy bandwidth; `cpu_baseline` is the CPU oracle (OpenMP over chunks) on a bounded
+sample of the same workload.  --impl reference times that CPU decoder as the reference arm
+(CODAG's own decoders exist only as GPU kernels; the oracle restates them on the CPU).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import time
+from datetime import timedelta
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+CH = 131072
+SEED = 20260101
+WORKLOADS = {
+    "rlev2": dict(codec=1, n=134_217_728, elem=8, desc="ORC RLE v2, 134,217,728 int64 (1 GiB), 8192 x 128 KiB chunks"),
+    "rlev1": dict(codec=0, n=1_048_576, elem=8, desc="ORC RLE v1, 1,048,576 uint64 (8 MiB), 64 x 128 KiB chunks"),
+    "rlev1x128": dict(codec=0, n=134_217_728, elem=8, desc="ORC RLE v1, 134,217,728 uint64 (1 GiB), 8192 x 128 KiB chunks"),
+    "deflate": dict(codec=2, n=1 << 30, elem=1, desc="Deflate (zlib level 6), 1 GiB Zipf text, 8192 x 128 KiB chunks"),
+}
+KERNEL_NAMES = {0: "k_rle_plain<.., RLEV1>", 1: "k_rle_plain<.., RLEV2>", 2: "k_inflate_plain"}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(workload: str):
+    """DRAM bytes per launch of the decode kernel from the committed ncu summary, if any."""
+    f = ROOT / "profiles" / "ncu_traffic.md"
+    if not f.exists():
+        return None
+    m = re.search(rf"^\|\s*{re.escape(workload)}\s*\|\s*([0-9]+)\s*\|", f.read_text(), re.M)
+    return int(m.group(1)) if m else None
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in Path(self.f.name).read_text().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if "Active" in v and "Not" not in v})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# --- workload construction (product format producers) -------------------------------------------
+def make_file(workload: str, rank: int):
+    from codag_b200 import native as nat
+    w = WORKLOADS[workload]
+    seed = SEED + 1000 * rank + w["codec"]
+    if w["codec"] == 0:
+        col = nat.gen_rlev1_column(w["n"], seed, w["elem"])
+        blob, off, ln = nat.encode_rlev1(col, CH, w["elem"])
+        return dict(col=col, comp=blob[8:], off=off[:ln.size], ln=ln)
+    if w["codec"] == 1:
+        col = nat.gen_rlev2_column(w["n"], seed, w["elem"])
+        comp, off, ln = nat.encode_rlev2(col, CH, w["elem"])
+        return dict(col=col, comp=comp, off=off[:ln.size], ln=ln)
+    txt = nat.gen_text(w["n"], seed)
+    comp, bo, cl = nat.encode_deflate(txt, CH, 6)
+    return dict(col=txt, comp=comp, off=bo[1:], ln=cl)
+
+
+def cpu_sample(f, codec: int, elem: int, max_chunks: int):
+    """Oracle decode of the first max_chunks chunks on all host threads; returns (GB/s, threads, desc)."""
+    from oracle import oracle_py
+    n = min(max_chunks, f["ln"].size)
+    if codec == 2:
+        comp_off, comp_len = f["off"][:n], np.diff(f["off"][:n + 1])
+        wrapper = [2] * n
+    else:
+        comp_off, comp_len = f["off"][:n], f["ln"][:n]
+        wrapper = [0] * n
+    out = np.empty(n * CH, np.uint8)
+    args = (f["comp"], comp_off, comp_len, out, np.arange(n, dtype=np.uint64) * CH, [CH] * n, [CH] * n,
+            [codec] * n, [elem] * n, wrapper)
+    oracle_py.decode_batch(*args)  # warm-up
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        st = oracle_py.decode_batch(*args)
+        times.append(time.perf_counter() - t0)
+        assert not st.any()
+    t = float(np.median(times))
+    return n * CH / t / 1e9, oracle_py.max_threads(), f"{n} chunks x 128 KiB ({n * CH / 2**20:.0f} MiB), median of 3"
+
+
+# --- arms ------------------------------------------------------------------------------------------
+def run_reference(args):
+    """CPU decoder of the path (oracle port, OpenMP over chunks) on a bounded sample per step."""
+    w = WORKLOADS[args.workload]
+    f = make_file(args.workload, 0)
+    sample = 1024 if w["codec"] != 2 else 256
+    from oracle import oracle_py
+    n = min(sample, f["ln"].size)
+    if w["codec"] == 2:
+        comp_off, comp_len, wrapper = f["off"][:n], np.diff(f["off"][:n + 1]), [2] * n
+    else:
+        comp_off, comp_len, wrapper = f["off"][:n], f["ln"][:n], [0] * n
+    out = np.empty(n * CH, np.uint8)
+    a = (f["comp"], comp_off, comp_len, out, np.arange(n, dtype=np.uint64) * CH, [CH] * n, [CH] * n,
+         [w["codec"]] * n, [w["elem"]] * n, wrapper)
+    for _ in range(args.warmup):
+        oracle_py.decode_batch(*a)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        st = oracle_py.decode_batch(*a)
+    dt = time.perf_counter() - t0
+    assert not st.any()
+    gbs = args.steps * n * CH / dt / 1e9
+    threads = oracle_py.max_threads()
+    desc = f"{n} chunks x 128 KiB of the workload per step ({n * CH / 2**20:.0f} MiB)"
+    line = {"metric": "decompressed GB/s", "value": round(gbs, 3), "unit": "GB/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8" if w["codec"] == 2 else "int64",
+            "data": "synthetic (seeded generators standing in for CODAG's datasets)",
+            "config": {"workload": w["desc"], "chunk_bytes": CH, "sample": desc},
+            "impl": "reference",
+            "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port", "sample": desc},
+            "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank: int, world: int, local: int):
+    import torch
+    import torch.distributed as dist
+    from codag_b200 import api, native as nat
+
+    torch.cuda.set_device(local)
+    w = WORKLOADS[args.workload]
+    codec, e = w["codec"], w["elem"]
+    f = make_file(args.workload, rank)
+    n = f["ln"].size
+    out_bytes = f["col"].size
+    comp_bytes = f["comp"].size
+    alg_bytes = int(f["ln"].sum()) + n * CH  # compressed stream bytes read + decompressed bytes written
+    dev = torch.device("cuda", local)
+
+    def t64(a):
+        return torch.from_numpy(np.ascontiguousarray(a).astype(np.uint64).view(np.int64)).to(dev)
+
+    d_comp = torch.from_numpy(f["comp"]).to(dev)
+    d_off, d_len = t64(f["off"]), t64(f["ln"])
+    d_out = torch.empty(n * CH, dtype=torch.uint8, device=dev)
+    d_st = torch.zeros(n, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def launch(comp=d_comp, off=d_off, ln=d_len, out=d_out, obytes=None):
+        if codec == 0:
+            api.decompress_rlev1(comp, off, ln, CH, e, out, obytes, d_st, stream)
+        elif codec == 1:
+            api.decompress_rlev2(comp, off, ln, CH, e, out, obytes, d_st, stream)
+        else:
+            api.decompress_deflate(comp, off, CH, out, 2, obytes, d_st, stream)
+
+    for _ in range(max(args.warmup, 3)):
+        launch()
+    torch.cuda.synchronize()
+    # correctness of the timed configuration (outside the timed region)
+    ok = int((d_st != 0).sum().item()) == 0 and bool(torch.equal(d_out[:out_bytes], torch.from_numpy(f["col"]).to(dev)))
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = Clocks(local) if rank == 0 else None
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
+    t_all0, t_all1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t_all0.record(stream)
+    for i in range(args.steps):
+        ev[i][0].record(stream)
+        launch()
+        ev[i][1].record(stream)
+    t_all1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop() if clocks else None
+    elapsed = t_all0.elapsed_time(t_all1) / 1e3
+    per_launch = float(np.mean([a.elapsed_time(b) for a, b in ev])) / 1e3
+    if world > 1:
+        t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+        okt = torch.tensor([0 if ok else 1], dtype=torch.int32, device=dev)
+        dist.all_reduce(okt)
+        ok = int(okt.item()) == 0
+
+    # e2e: host buffers in pinned memory, copies inside the timed region
+    h_comp = torch.from_numpy(f["comp"]).pin_memory()
+    h_off = torch.from_numpy(f["off"].astype(np.uint64).view(np.int64)).pin_memory()
+    h_len = torch.from_numpy(f["ln"].astype(np.uint64).view(np.int64)).pin_memory()
+    h_out = torch.empty(out_bytes, dtype=torch.uint8).pin_memory()
+    e_comp = torch.empty_like(d_comp)
+    e_off, e_len = torch.empty_like(d_off), torch.empty_like(d_len)
+    e_steps = max(2, min(args.steps, 5))
+    h2d_bytes = h_comp.numel() + 8 * h_off.numel() + (8 * h_len.numel() if codec != 2 else 0)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e_steps):
+        e_comp.copy_(h_comp, non_blocking=True)
+        e_off.copy_(h_off, non_blocking=True)
+        if codec != 2:
+            e_len.copy_(h_len, non_blocking=True)
+        launch(e_comp, e_off, e_len, d_out, out_bytes)
+        h_out.copy_(d_out[:out_bytes], non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_t = e0.elapsed_time(e1) / 1e3
+    if world > 1:
+        t = torch.tensor([e2e_t], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
+    ok = ok and bool(torch.equal(h_out, torch.from_numpy(f["col"])))
+
+    if rank != 0:
+        return
+    peak, peak_kind = peaks()
+    achieved = alg_bytes / per_launch / 1e9
+    launches = args.steps
+    value = world * out_bytes * args.steps / elapsed / 1e9
+    traffic = ncu_traffic(args.workload)
+    cpu = None
+    if world == 1:
+        gbs, threads, desc = cpu_sample(f, codec, e, 1024 if codec != 2 else 256)
+        cpu = {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port", "sample": desc}
+    line = {
+        "metric": "decompressed GB/s", "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(elapsed / args.steps * 1e3, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8" if codec == 2 else "int64",
+        "data": "synthetic (seeded generators standing in for CODAG's datasets)",
+        "config": {"workload": w["desc"], "chunk_bytes": CH, "n_chunks": n, "comp_bytes": comp_bytes,
+                   "out_bytes": out_bytes, "l2": "inputs larger than L2 (no flush)",
+                   "parallelism": f"{world} GPU(s), chunks per GPU independent",
+                   "tune": {k: getattr(nat.get_tune(codec), k) for k in ("warps_per_cta", "ring_slots", "lut_bits")}},
+        "bit_exact": ok,
+        "e2e": {"value": round(world * out_bytes * e_steps / e2e_t / 1e9, 2), "unit": "GB/s",
+                "h2d_bytes_per_step": int(h2d_bytes), "d2h_bytes_per_step": int(out_bytes)},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": KERNEL_NAMES[codec], "alg_bytes_per_launch": alg_bytes,
+                     "launch_ms": round(per_launch * 1e3, 4)},
+        "cpu_baseline": cpu,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="rlev2", choices=sorted(WORKLOADS) + ["batched"])
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == "batched":
+        from codag_b200 import batched_bench
+        return batched_bench.main(args, rank, world, local)
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args)
+        return
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    try:
+        run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

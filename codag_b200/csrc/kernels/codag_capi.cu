@@ -335,6 +335,9 @@ extern "C" codag_status codag_set_tune(int codec, const codag_tune* tune) {
   if (codec < 0 || codec > 2 || !tune || !valid_warps(tune->warps_per_cta) || !valid_slots(tune->ring_slots) ||
       !valid_lut(tune->lut_bits))
     return CODAG_EINVAL;
+  // an RLE v2 header with its data spans up to 2060 bytes; it must fit the window of
+  // (slots - 1) KiB ahead of the read position
+  if (codec != CODAG_CODEC_DEFLATE && tune->ring_slots < 4) return CODAG_EINVAL;
   std::lock_guard<std::mutex> g(g_mu);
   g_tune[codec] = *tune;
   return CODAG_OK;
@@ -454,6 +457,7 @@ extern "C" codag_status codag_batch_plan(const codag_chunk_desc* h_descs, uint64
   if (!h_descs || !plan || n == 0 || n > 0xffffffffull) return CODAG_EINVAL;
   codag_tune t = tune ? *tune : tune_of(CODAG_CODEC_DEFLATE);
   if (!valid_warps(t.warps_per_cta) || !valid_slots(t.ring_slots) || !valid_lut(t.lut_bits)) return CODAG_EINVAL;
+  if (t.ring_slots < 4) t.ring_slots = 4;  // mixed batches include RLE chunks
   for (uint64_t i = 0; i < n; i++) {
     const codag_chunk_desc& d = h_descs[i];
     if (d.codec > CODAG_CODEC_DEFLATE) return CODAG_EINVAL;

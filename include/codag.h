@@ -84,8 +84,9 @@ codag_status codag_decompress_deflate(const uint8_t *d_comp, uint64_t comp_bytes
 
 /* --- launch tuning --------------------------------------------------------------------
  * Process-wide launch shape for the per-file calls above, per codec.  warps_per_cta is
- * the number of chunks one CTA decodes (one warp per chunk); ring_slots the depth of the
- * TMA input ring (2, 4 or 8 slots of 1 KiB); lut_bits the primary Huffman table width
+ * the number of chunks one CTA decodes (one warp per chunk, 1..8); ring_slots the depth of
+ * the TMA input ring (2, 4 or 8 slots of 1 KiB; the RLE codecs need at least 4 because an
+ * RLE v2 header with its data spans up to 2060 bytes); lut_bits the primary Huffman table width
  * (Deflate only: 9, 10 or 11).  Values outside the supported sets return CODAG_EINVAL. */
 typedef struct {
     int32_t warps_per_cta;
