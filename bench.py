@@ -105,9 +105,11 @@ class Clocks:
 
 
 # --- workload construction (product format producers) -------------------------------------------
-def make_file(workload: str, rank: int):
+def make_file(workload: str, rank: int, n_values: int | None = None):
     from codag_b200 import native as nat
-    w = WORKLOADS[workload]
+    w = dict(WORKLOADS[workload])
+    if n_values:
+        w["n"] = n_values
     seed = SEED + 1000 * rank + w["codec"]
     if w["codec"] == 0:
         col = nat.gen_rlev1_column(w["n"], seed, w["elem"])
@@ -150,7 +152,7 @@ def cpu_sample(f, codec: int, elem: int, max_chunks: int):
 def run_reference(args):
     """CPU decoder of the path (oracle port, OpenMP over chunks) on a bounded sample per step."""
     w = WORKLOADS[args.workload]
-    f = make_file(args.workload, 0)
+    f = make_file(args.workload, 0, args.n_values)
     sample = 1024 if w["codec"] != 2 else 256
     from oracle import oracle_py
     n = min(sample, f["ln"].size)
@@ -190,7 +192,7 @@ def run_ours(args, rank: int, world: int, local: int):
     torch.cuda.set_device(local)
     w = WORKLOADS[args.workload]
     codec, e = w["codec"], w["elem"]
-    f = make_file(args.workload, rank)
+    f = make_file(args.workload, rank, args.n_values)
     n = f["ln"].size
     out_bytes = f["col"].size
     comp_bytes = f["comp"].size
@@ -296,7 +298,8 @@ def run_ours(args, rank: int, world: int, local: int):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u8" if codec == 2 else "int64",
         "data": "synthetic (seeded generators standing in for CODAG's datasets)",
-        "config": {"workload": w["desc"], "chunk_bytes": CH, "n_chunks": n, "comp_bytes": comp_bytes,
+        "config": {"workload": w["desc"] if not args.n_values else f"{w['desc']} resized to {args.n_values} values",
+                   "chunk_bytes": CH, "n_chunks": n, "comp_bytes": comp_bytes,
                    "out_bytes": out_bytes, "l2": "inputs larger than L2 (no flush)",
                    "parallelism": f"{world} GPU(s), chunks per GPU independent",
                    "tune": {k: getattr(nat.get_tune(codec), k) for k in ("warps_per_cta", "ring_slots", "lut_bits")}},
@@ -321,6 +324,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="rlev2", choices=sorted(WORKLOADS) + ["batched"])
+    ap.add_argument("--n-values", type=int, default=None,
+                    help="override the workload's element count (profiling cases; not a bench line)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -122,8 +122,10 @@ def test_rle_malformed_streams(native, cuda, api):
     assert st[1] == 2 and st[2] == 2
     ok = [i for i in range(ln.size) if i not in (1, 2)]
     assert not st[ok].any()
+    padded = np.zeros(ln.size * CH, np.uint8)  # chunks past the column hold the layout's zero padding
+    padded[:col.size] = col
     for i in ok:
-        assert np.array_equal(out[i * CH:(i + 1) * CH], col[i * CH:(i + 1) * CH])
+        assert np.array_equal(out[i * CH:(i + 1) * CH], padded[i * CH:(i + 1) * CH])
     # RLE v1: random garbage bytes never fault and never write past their chunk
     rng = np.random.default_rng(7)
     garbage = rng.integers(0, 256, size=64 * 1024, dtype=np.uint8)
@@ -140,7 +142,7 @@ def test_rle_stream_out_of_bounds(native, cuda, api):
     off = off.copy()
     off[1] = comp.size + 100  # beyond comp_bytes
     st, _ = _gpu_rle(cuda, api, RLEV2, comp, off, ln, CH, 8)
-    assert st.tolist() == [0, 2]
+    assert st[1] == 2 and not np.delete(st, 1).any()
 
 
 # --- Deflate -------------------------------------------------------------------------------------
