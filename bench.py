@@ -216,6 +216,9 @@ def run_ours(args, rank: int, world: int, local: int):
         else:
             api.decompress_deflate(comp, off, CH, out, 2, obytes, d_st, stream)
 
+    if args.autotune:
+        from codag_b200 import tuning
+        best, res = tuning.autotune(codec, launch, use_cache=args.autotune == "cached", verbose=rank == 0)
     for _ in range(max(args.warmup, 3)):
         launch()
     torch.cuda.synchronize()
@@ -324,6 +327,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="rlev2", choices=sorted(WORKLOADS) + ["batched"])
+    ap.add_argument("--autotune", default="cached", choices=["cached", "search", ""],
+                    help="pick the launch shape with the autotuner (cached result or a fresh search)")
     ap.add_argument("--n-values", type=int, default=None,
                     help="override the workload's element count (profiling cases; not a bench line)")
     args = ap.parse_args()

@@ -60,11 +60,11 @@ __device__ __forceinline__ bool stream_in_bounds(uint64_t off, uint64_t len, uin
 // ---------------------------------------------------------------------------------------
 // plain kernels: chunk = blockIdx.x * warps + warp
 // ---------------------------------------------------------------------------------------
-template <int NSLOT, int CODEC>
+template <int NSLOT, int CODEC, int E>
 __global__ void __launch_bounds__(256) k_rle_plain(const uint8_t* __restrict__ comp, uint64_t comp_bytes,
                                                    const uint64_t* __restrict__ blk_off,
                                                    const uint64_t* __restrict__ col_len, uint64_t n_chunks,
-                                                   uint64_t chunk_bytes, int e, uint8_t* __restrict__ out,
+                                                   uint64_t chunk_bytes, uint8_t* __restrict__ out,
                                                    uint64_t out_bytes, int32_t* __restrict__ status,
                                                    uint64_t wait_cycles) {
   extern __shared__ __align__(128) uint8_t smem[];
@@ -92,8 +92,8 @@ __global__ void __launch_bounds__(256) k_rle_plain(const uint8_t* __restrict__ c
   } else {
     in.begin(comp + off, static_cast<uint32_t>(len));
     o.begin(out + cbase, store_bytes(cbase, chunk_bytes, out_bytes));
-    st = CODEC == CODAG_CODEC_RLEV1 ? decode_rlev1_chunk<NSLOT>(in, o, chunk_bytes, e)
-                                    : decode_rlev2_chunk<NSLOT>(in, o, chunk_bytes, e);
+    const uint32_t cap = static_cast<uint32_t>(chunk_bytes / E);
+    st = CODEC == CODAG_CODEC_RLEV1 ? decode_rlev1_chunk<NSLOT, E>(in, o, cap) : decode_rlev2_chunk<NSLOT, E>(in, o, cap);
   }
   if (status && lane == 0) status[chunk] = st;
 }
@@ -175,8 +175,8 @@ __global__ void __launch_bounds__(256) k_batch(const codag_chunk_desc* __restric
       in.begin(comp + d.comp_off, d.comp_len);
       o.begin(out + d.out_off, d.out_len);
       switch (d.codec) {
-        case CODAG_CODEC_RLEV1: st = decode_rlev1_chunk<NSLOT>(in, o, d.out_len, d.elem_bytes); break;
-        case CODAG_CODEC_RLEV2: st = decode_rlev2_chunk<NSLOT>(in, o, d.out_len, d.elem_bytes); break;
+        case CODAG_CODEC_RLEV1:
+        case CODAG_CODEC_RLEV2: st = decode_rle_any<NSLOT>(d.codec, in, o, d.out_len, d.elem_bytes); break;
         case CODAG_CODEC_DEFLATE: st = decode_deflate_chunk<NSLOT, LB>(in, o, sc, d.out_len, d.wrapper_bytes); break;
         default: st = CODAG_EINVAL;
       }
@@ -235,20 +235,32 @@ codag_status finish_launch() {
   return err == cudaSuccess ? CODAG_OK : CODAG_ECUDA;
 }
 
-template <int NSLOT, int CODEC>
+template <int NSLOT, int CODEC, int E>
 codag_status launch_rle(const codag_tune& t, const uint8_t* comp, uint64_t comp_bytes, const uint64_t* blk_off,
-                        const uint64_t* col_len, uint64_t n, uint64_t chunk_bytes, int e, uint8_t* out,
-                        uint64_t out_bytes, int32_t* status, cudaStream_t s) {
+                        const uint64_t* col_len, uint64_t n, uint64_t chunk_bytes, uint8_t* out, uint64_t out_bytes,
+                        int32_t* status, cudaStream_t s) {
   using L = RleLayout<NSLOT>;
   const uint32_t smem = L::kPerWarp * t.warps_per_cta;
-  auto kern = k_rle_plain<NSLOT, CODEC>;
+  auto kern = k_rle_plain<NSLOT, CODEC, E>;
   if (allow_smem(kern, smem) != cudaSuccess) return CODAG_ECUDA;
   const uint64_t grid = (n + t.warps_per_cta - 1) / t.warps_per_cta;
   if (grid > 0x7fffffffull) return CODAG_EINVAL;
   kern<<<static_cast<unsigned>(grid), 32 * t.warps_per_cta, smem, s>>>(comp, comp_bytes, blk_off, col_len, n,
-                                                                         chunk_bytes, e, out, out_bytes, status,
+                                                                         chunk_bytes, out, out_bytes, status,
                                                                          wait_of());
   return finish_launch();
+}
+
+template <int NSLOT, int CODEC>
+codag_status launch_rle_e(const codag_tune& t, const uint8_t* comp, uint64_t comp_bytes, const uint64_t* blk_off,
+                          const uint64_t* col_len, uint64_t n, uint64_t chunk_bytes, int e, uint8_t* out,
+                          uint64_t out_bytes, int32_t* status, cudaStream_t s) {
+  switch (e) {
+    case 8: return launch_rle<NSLOT, CODEC, 8>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, out, out_bytes, status, s);
+    case 4: return launch_rle<NSLOT, CODEC, 4>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, out, out_bytes, status, s);
+    case 2: return launch_rle<NSLOT, CODEC, 2>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, out, out_bytes, status, s);
+    default: return launch_rle<NSLOT, CODEC, 1>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, out, out_bytes, status, s);
+  }
 }
 
 template <int NSLOT, int LB>
@@ -272,15 +284,13 @@ codag_status dispatch_rle(const uint8_t* comp, uint64_t comp_bytes, const uint64
                           uint64_t n, uint64_t chunk_bytes, int e, uint8_t* out, uint64_t out_bytes, int32_t* status,
                           cudaStream_t s) {
   if (!comp || !blk_off || !col_len || (!out && out_bytes) || !valid_elem(e) || chunk_bytes == 0 ||
-      chunk_bytes % static_cast<uint64_t>(e))
+      chunk_bytes % static_cast<uint64_t>(e) || chunk_bytes >= (1ull << 31))
     return CODAG_EINVAL;
   if (n == 0) return CODAG_OK;
   const codag_tune t = tune_of(CODEC);
-  switch (t.ring_slots) {
-    case 2: return launch_rle<2, CODEC>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, e, out, out_bytes, status, s);
-    case 4: return launch_rle<4, CODEC>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, e, out, out_bytes, status, s);
-    default: return launch_rle<8, CODEC>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, e, out, out_bytes, status, s);
-  }
+  if (t.ring_slots == 4)
+    return launch_rle_e<4, CODEC>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, e, out, out_bytes, status, s);
+  return launch_rle_e<8, CODEC>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, e, out, out_bytes, status, s);
 }
 
 }  // namespace

@@ -1,261 +1,367 @@
 // Warp decoders for ORC RLE v1 and ORC RLE v2 chunks.
 //
-// CODAG decodes these with one lane walking the stream byte by byte and the other 31 lanes
-// idle or storing the same addresses (include/rlev1/decoder.h:588-798,
+// CODAG decodes these with one lane walking the stream byte by byte while the other lanes
+// idle or store the same addresses (include/rlev1/decoder.h:588-798,
 // include/rlev2/decoder_new.h:909-1187).  Here the header walk stays sequential (each
-// header's size depends on its contents) but everything inside a header is lane-parallel:
-//   RLE v1  literal groups: 32 stream bytes per step, varint ends found with one ballot of
-//           the byte MSBs, values assembled by a segmented OR scan; runs: one value per lane.
-//   RLE v2  DIRECT/PATCHED_BASE values unpacked one per lane by direct bit addressing;
-//           DELTA deltas unpacked one per lane and accumulated with a warp scan;
-//           PATCHED_BASE patch gaps accumulated with a warp scan and applied by the first
-//           lane of each group of patches that hit the same value.
-// Decoded values go to the shared-memory output ring (OutRing) and leave it as 16-byte stores.
-// Arithmetic on values is modulo 2^(8*elem_bytes), with the reference's quirks kept
-// (see oracle/oracle.c for the list).
+// header's size depends on its contents) but is kept to a few dozen warp instructions per
+// header, and everything inside a header is lane-parallel:
+//   - headers are read with one 8-byte big-endian peek; LEB128 varints are decoded in
+//     registers by compacting the 7-bit groups of an 8- or 16-byte window;
+//   - RLE v1 literal groups are scanned 128 bytes per step, 4 bytes per lane: one ballot per
+//     byte lane finds the varint ends, and the lane holding an end decodes that varint;
+//   - RLE v1 runs and RLE v2 SHORT_REPEAT/fixed-step DELTA values are produced one per lane;
+//   - RLE v2 DIRECT/PATCHED_BASE values are unpacked one per lane by direct bit addressing
+//     (two or three aligned shared-memory words and a funnel shift);
+//   - RLE v2 packed DELTA deltas are accumulated with a warp scan;
+//   - PATCHED_BASE patch offsets are prefix-summed across the patch lanes and applied by
+//     those lanes (a group of patches hitting one value is OR-combined first).
+// Decoded values go to the shared-memory output ring (OutRing) and leave it as 16-byte
+// stores.  Element arithmetic is modulo 2^(8*E), keeping the reference's quirks (see
+// oracle/oracle.c for the list).
 #pragma once
 #include "device_common.cuh"
 
 namespace codag_dev {
 
-__device__ __forceinline__ uint64_t elem_mask(int e) { return e == 8 ? ~0ull : ((1ull << (8 * e)) - 1ull); }
+template <int E>
+struct ElemType;
+template <>
+struct ElemType<1> { using T = uint8_t; };
+template <>
+struct ElemType<2> { using T = uint16_t; };
+template <>
+struct ElemType<4> { using T = uint32_t; };
+template <>
+struct ElemType<8> { using T = uint64_t; };
 
-__constant__ uint8_t kV2WidthDecode[32] = {1,  2,  3,  4,  5,  6,  7,  8,  9,  10, 11,
-                                           12, 13, 14, 15, 16, 17, 18, 19, 20, 21, 22,
-                                           23, 24, 26, 28, 30, 32, 40, 48, 56, 64};
-__constant__ uint8_t kV2Closest[65] = {
-    1,  1,  2,  3,  4,  5,  6,  7,  8,  9,  10, 11, 12, 13, 14, 15, 16, 17, 18, 19, 20, 21,
-    22, 23, 24, 26, 26, 28, 28, 30, 30, 32, 32, 40, 40, 40, 40, 40, 40, 40, 40, 48, 48, 48,
-    48, 48, 48, 48, 48, 56, 56, 56, 56, 56, 56, 56, 56, 64, 64, 64, 64, 64, 64, 64, 64};
+template <int E>
+__device__ __forceinline__ constexpr uint64_t emask() {
+  return E == 8 ? ~0ull : ((1ull << (8 * E)) - 1ull);
+}
+
+template <int E, class OUT>
+__device__ __forceinline__ void put_elem(OUT& o, uint32_t idx, uint64_t v) {
+  using T = typename ElemType<E>::T;
+  *reinterpret_cast<T*>(o.buf + ((idx * static_cast<uint32_t>(E)) & OUT::kMask)) = static_cast<T>(v);
+}
+
+template <int E, class OUT>
+__device__ __forceinline__ uint64_t get_elem(const OUT& o, uint32_t idx) {
+  using T = typename ElemType<E>::T;
+  return *reinterpret_cast<const T*>(o.buf + ((idx * static_cast<uint32_t>(E)) & OUT::kMask));
+}
+
+// bit width of a 5-bit width code (include/rlev2/utils.h:28)
+__device__ __forceinline__ uint32_t v2_width(uint32_t c) {
+  return c < 24 ? c + 1 : (c < 28 ? 2 * c - 22 : 8 * c - 184);
+}
+// smallest representable width >= b, for b in 0..64 (utils.h:42-48)
+__device__ __forceinline__ uint32_t v2_closest(uint32_t b) {
+  return b <= 24 ? (b ? b : 1u) : (b <= 32 ? (b + 1) & ~1u : (b + 7) & ~7u);
+}
+
+// LEB128 payload of the first `len` bytes of a little-endian window (len 1..8)
+__device__ __forceinline__ uint64_t leb_compact(uint64_t x, uint32_t len) {
+  if (len < 8) x &= (1ull << (8 * len)) - 1ull;
+  x &= 0x7F7F7F7F7F7F7F7Full;
+  x = (x & 0x007F007F007F007Full) | ((x >> 1) & 0x3F803F803F803F80ull);
+  x = (x & 0x00003FFF00003FFFull) | ((x >> 2) & 0x0FFFC0000FFFC000ull);
+  x = (x & 0x000000000FFFFFFFull) | ((x >> 4) & 0x00FFFFFFF0000000ull);
+  return x;
+}
+// value of a LEB128 varint of `len` bytes whose first 16 bytes are lo8, hi8; bytes past
+// the 10th only feed bits above 63 and vanish, as with the reference's clamped shifts
+__device__ __forceinline__ uint64_t leb_value(uint64_t lo8, uint64_t hi8, uint32_t len) {
+  if (len <= 8) return leb_compact(lo8, len);
+  return leb_compact(lo8, 8) | (leb_compact(hi8, len - 8 < 8 ? len - 8 : 8) << 56);
+}
+
+// Reads the unsigned varint at `p` (all lanes, same data); false if it is truncated or
+// longer than the resident window allows (1 KiB).
+template <int NSLOT>
+__device__ __forceinline__ bool read_uvarint(InRing<NSLOT>& in, uint32_t p, uint32_t end, uint32_t& len,
+                                             uint64_t& val) {
+  if (p + 20 > in.ready && in.ensure(min(p + 20, end))) return false;
+  const uint64_t lo8 = in.peek_le64(p);
+  uint64_t t = ~lo8 & 0x8080808080808080ull;
+  if (t) {
+    len = (static_cast<uint32_t>(__ffsll(t)) >> 3);
+    val = leb_compact(lo8, len);
+  } else {
+    const uint64_t hi8 = in.peek_le64(p + 8);
+    t = ~hi8 & 0x8080808080808080ull;
+    if (t) {
+      len = 8 + (static_cast<uint32_t>(__ffsll(t)) >> 3);
+      val = leb_value(lo8, hi8, len);
+    } else {  // longer than 16 bytes: only the first 16 carry bits; find the end
+      uint32_t q = p + 16;
+      const uint32_t lim = min(end, p + 1024);
+      if (in.ensure(lim)) return false;
+      while (q < lim && in.rd8(q) >= 0x80u) q++;
+      if (q >= lim) return false;
+      len = q - p + 1;
+      val = leb_value(lo8, hi8, len);
+    }
+  }
+  return p + len <= end;
+}
 
 // ---------------------------------------------------------------------------------------
 // ORC RLE v1
 // ---------------------------------------------------------------------------------------
-// Decodes one chunk.  Loops while fewer than chunk_bytes bytes were produced, as the
-// reference does (decoder.h:669).
-template <int NSLOT, class OUT>
-__device__ int decode_rlev1_chunk(InRing<NSLOT>& in, OUT& out, uint64_t chunk_bytes, int e) {
+// Decodes one chunk of `cap` elements.  Loops while fewer than cap elements were produced,
+// as the reference does (decoder.h:669).
+template <int NSLOT, int E, class OUT>
+__device__ int decode_rlev1_chunk(InRing<NSLOT>& in, OUT& out, uint32_t cap) {
+  constexpr uint64_t M = emask<E>();
   const uint32_t lane = in.lane;
-  const uint64_t m = elem_mask(e);
-  const uint64_t cap = chunk_bytes / static_cast<uint32_t>(e);
-  uint32_t pos = in.lo;
   const uint32_t end = in.hi;
-  uint64_t n = 0;
+  uint32_t pos = in.lo;
+  uint32_t n = 0;
   int st = CODAG_OK;
 
   while (n < cap) {
     if (pos >= end) { st = CODAG_ECORRUPT; break; }
-    if (!in.release(pos)) { st = CODAG_ETIMEOUT; break; }
-    // header, delta and base varint, or the start of a literal group
-    st = in.ensure(min(pos + 34, end));
+    st = in.advance(pos, min(pos + 32, end));
     if (st) break;
-    const int h = static_cast<int8_t>(in.rd8(pos));
+    const uint32_t head = in.rd8(pos);
+    const int h = static_cast<int8_t>(head);
     if (h >= 0) {
       // run: count h+3, int8 delta, varint base (decoder.h:731-790)
       if (pos + 2 >= end) { st = CODAG_ECORRUPT; break; }
       const int64_t delta = static_cast<int8_t>(in.rd8(pos + 1));
-      const uint32_t q = pos + 2 + lane;
-      const uint32_t b = q < end ? in.rd8(q) : 0x80u;
-      const uint32_t term = __ballot_sync(FULL, b < 0x80u);
-      if (!term) { st = CODAG_ECORRUPT; break; }
-      const uint32_t len = __ffs(term);  // bytes of the base varint
-      const uint64_t base = warp_or64(lane < len ? shl64(b & 0x7fu, 7u * lane) : 0ull);
+      uint32_t len;
+      uint64_t base;
+      if (!read_uvarint(in, pos + 2, end, len, base)) { st = CODAG_ECORRUPT; break; }
       const uint32_t cnt = static_cast<uint32_t>(h) + 3u;
       if (n + cnt > cap) { st = CODAG_ECORRUPT; break; }
-      for (uint32_t i = lane; i < cnt; i += 32)
-        out.put(n + i, (base + static_cast<uint64_t>(static_cast<int64_t>(i) * delta)) & m, e);
+      uint64_t v = base + static_cast<uint64_t>(static_cast<int64_t>(lane) * delta);
+      const uint64_t step = static_cast<uint64_t>(32 * delta);
+      for (uint32_t i = lane; i < cnt; i += 32, v += step) put_elem<E>(out, n + i, v & M);
       n += cnt;
       pos += 2 + len;
     } else {
-      // literal group of -h varints (decoder.h:686-727)
+      // literal group of -h varints (decoder.h:686-727), 128 stream bytes per step
       uint32_t remaining = static_cast<uint32_t>(-h);
       if (n + remaining > cap) { st = CODAG_ECORRUPT; break; }
       pos += 1;
       while (remaining) {
-        if (!in.release(pos)) { st = CODAG_ETIMEOUT; break; }
-        st = in.ensure(min(pos + 32, end));
+        st = in.advance(pos, min(pos + 148, end));
         if (st) break;
-        const uint32_t q = pos + lane;
-        const bool valid = q < end;
-        const uint32_t b = valid ? in.rd8(q) : 0x80u;
-        const uint32_t term = __ballot_sync(FULL, valid && b < 0x80u);
-        if (!term) { st = CODAG_ECORRUPT; break; }
-        // byte `lane` belongs to varint number `seg`, which started after the previous end
-        const uint32_t below = term & lanemask_lt(lane);
-        const uint32_t seg = __popc(below);
-        const uint32_t start = below ? 32u - __clz(below) : 0u;
-        uint64_t v = shl64(b & 0x7fu, 7u * (lane - start));
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {  // segmented inclusive OR scan
-          const uint64_t o = shfl_up64(v, d);
-          const uint32_t oseg = __shfl_up_sync(FULL, seg, d);
-          if (lane >= static_cast<uint32_t>(d) && oseg == seg) v |= o;
+        const uint32_t q0 = pos + 4 * lane;
+        const uint32_t w4 = static_cast<uint32_t>(in.peek_le64(q0));
+        const uint32_t tb = ~w4 & 0x80808080u;
+        uint32_t nib = ((tb >> 7) & 1u) | ((tb >> 14) & 2u) | ((tb >> 21) & 4u) | ((tb >> 28) & 8u);
+        if (q0 + 4 > end) nib &= q0 >= end ? 0u : ((1u << (end - q0)) - 1u);
+        const uint32_t b0 = __ballot_sync(FULL, nib & 1u), b1 = __ballot_sync(FULL, nib & 2u);
+        const uint32_t b2 = __ballot_sync(FULL, nib & 4u), b3 = __ballot_sync(FULL, nib & 8u);
+        const uint32_t lt = lanemask_lt(lane);
+        const uint32_t before = __popc(b0 & lt) + __popc(b1 & lt) + __popc(b2 & lt) + __popc(b3 & lt);
+        const uint32_t total = __popc(b0) + __popc(b1) + __popc(b2) + __popc(b3);
+        if (!total) { st = CODAG_ECORRUPT; break; }  // a varint longer than 128 bytes
+        const uint32_t take = total < remaining ? total : remaining;
+        // end of the previous varint: the last end in a lower lane, or the window start
+        const uint32_t nz = __ballot_sync(FULL, nib != 0) & lt;
+        const uint32_t src = nz ? 31u - __clz(nz) : lane;
+        const uint32_t pnib = __shfl_sync(FULL, nib, src);
+        uint32_t start = nz ? pos + 4 * src + (32u - __clz(pnib)) : pos;
+        uint32_t m = nib, idx = before, last_end = 0;
+        while (m) {
+          const uint32_t q = q0 + __ffs(m) - 1;
+          m &= m - 1;
+          if (idx < take) {
+            const uint32_t len = q - start + 1;
+            const uint64_t lo8 = in.peek_le64(start);
+            const uint64_t hi8 = len > 8 ? in.peek_le64(start + 8) : 0ull;
+            put_elem<E>(out, n + idx, leb_value(lo8, hi8, len) & M);
+            if (idx == take - 1) last_end = q + 1;
+          }
+          idx++;
+          start = q + 1;
         }
-        const uint32_t avail = __popc(term);
-        const uint32_t take = avail < remaining ? avail : remaining;
-        if (((term >> lane) & 1u) && seg < take) out.put(n + seg, v & m, e);
-        // position after the take-th varint end
-        const uint32_t last_end = __ballot_sync(FULL, ((term >> lane) & 1u) && seg == take - 1u);
-        pos += static_cast<uint32_t>(__ffs(last_end));
+        pos = __reduce_max_sync(FULL, last_end);
         n += take;
         remaining -= take;
-        __syncwarp();
-        out.flush_to(n * static_cast<uint32_t>(e));
       }
       if (st) break;
     }
     __syncwarp();
-    out.flush_to(n * static_cast<uint32_t>(e));
+    out.flush_to(static_cast<uint64_t>(n) * E);
   }
   if (!in.drain() && st == CODAG_OK) st = CODAG_ETIMEOUT;
-  out.finish(n * static_cast<uint32_t>(e));
-  if (st == CODAG_OK && n * static_cast<uint32_t>(e) < out.store) st = CODAG_ECORRUPT;
+  out.finish(static_cast<uint64_t>(n) * E);
+  if (st == CODAG_OK && static_cast<uint64_t>(n) * E < out.store) st = CODAG_ECORRUPT;
   return st;
 }
 
 // ---------------------------------------------------------------------------------------
 // ORC RLE v2 (unsigned values, include/rlev2/decoder_new.h:909-1187)
 // ---------------------------------------------------------------------------------------
-template <int NSLOT, class OUT>
-__device__ int decode_rlev2_chunk(InRing<NSLOT>& in, OUT& out, uint64_t chunk_bytes, int e) {
+template <int NSLOT, int E, class OUT>
+__device__ int decode_rlev2_chunk(InRing<NSLOT>& in, OUT& out, uint32_t cap) {
+  constexpr uint64_t M = emask<E>();
   const uint32_t lane = in.lane;
-  const uint64_t m = elem_mask(e);
-  const uint64_t cap = chunk_bytes / static_cast<uint32_t>(e);
-  uint32_t pos = in.lo;
   const uint32_t end = in.hi;
-  uint64_t n = 0;
+  uint32_t pos = in.lo;
+  uint32_t n = 0;
   int st = CODAG_OK;
 
   while (pos < end) {
-    if (!in.release(pos)) { st = CODAG_ETIMEOUT; break; }
-    st = in.ensure(min(pos + 32, end));
+    st = in.advance(pos, min(pos + 32, end));
     if (st) break;
     const uint64_t hdr = in.peek_be64(pos);
     const uint32_t first = static_cast<uint32_t>(hdr >> 56);
-    const uint32_t second = static_cast<uint32_t>(hdr >> 48) & 0xffu;
-    const uint32_t kind = first & 0xC0u;
     // the length field is held in a uint8_t (decoder_new.h:1019,1048,1095)
-    const uint32_t len8 = ((((first & 1u) << 8) | second) + 1u) & 0xffu;
+    const uint32_t len8 = ((static_cast<uint32_t>(hdr >> 48) & 0x1ffu) + 1u) & 0xffu;
+    uint32_t cnt, total;
 
-    if (kind == 0x00u) {  // SHORT_REPEAT (decoder_new.h:1004-1014)
+    if ((first >> 6) == 0) {  // SHORT_REPEAT (decoder_new.h:1004-1014)
       const uint32_t nb = ((first >> 3) & 7u) + 1u;
-      const uint32_t cnt = (first & 7u) + 3u;
-      if (pos + 1 + nb > end) { st = CODAG_ECORRUPT; break; }
-      if (n + cnt > cap) { st = CODAG_ECORRUPT; break; }
-      const uint64_t v = (in.peek_be64(pos + 1) >> (64u - 8u * nb)) & m;
-      if (lane < cnt) out.put(n + lane, v, e);
-      n += cnt;
-      pos += 1 + nb;
-    } else if (kind == 0x40u) {  // DIRECT (decoder_new.h:1015-1043)
-      const uint32_t fbw = kV2WidthDecode[(first >> 1) & 0x1fu];
-      const uint32_t total = 2u + (len8 * fbw + 7u) / 8u;
-      if (pos + total > end || n + len8 > cap) { st = CODAG_ECORRUPT; break; }
-      st = in.ensure(pos + total);
+      cnt = (first & 7u) + 3u;
+      total = 1u + nb;
+      if (pos + total > end || n + cnt > cap) { st = CODAG_ECORRUPT; break; }
+      const uint64_t v = nb < 8 ? (hdr << 8) >> (64u - 8u * nb) : in.peek_be64(pos + 1);
+      if (lane < cnt) put_elem<E>(out, n + lane, v & M);
+    } else if ((first >> 6) == 1) {  // DIRECT (decoder_new.h:1015-1043)
+      const uint32_t fbw = v2_width((first >> 1) & 0x1fu);
+      cnt = len8;
+      total = 2u + (len8 * fbw + 7u) / 8u;
+      if (pos + total > end || n + cnt > cap) { st = CODAG_ECORRUPT; break; }
+      st = in.advance(pos, pos + total);
       if (st) break;
       const uint32_t bit0 = (pos + 2u) * 8u;
-      for (uint32_t j = lane; j < len8; j += 32) out.put(n + j, in.bits_be(bit0 + j * fbw, fbw) & m, e);
-      n += len8;
-      pos += total;
-    } else if (kind == 0xC0u) {  // DELTA (decoder_new.h:1044-1091)
+      if (fbw <= 32) {
+        for (uint32_t j = lane; j < cnt; j += 32) put_elem<E>(out, n + j, in.msb_bits32(bit0 + j * fbw, fbw) & M);
+      } else {
+        for (uint32_t j = lane; j < cnt; j += 32) put_elem<E>(out, n + j, in.msb_bits64(bit0 + j * fbw, fbw) & M);
+      }
+    } else if ((first >> 6) == 3) {  // DELTA (decoder_new.h:1044-1091)
       const uint32_t enc = (first >> 1) & 0x1fu;
-      const uint32_t fbw = kV2WidthDecode[enc];
-      // base (unsigned varint) and base delta (signed varint), one byte per lane
-      const uint32_t q = pos + 2 + lane;
-      const uint32_t b = (lane < 30 && q < end) ? in.rd8(q) : 0x80u;
-      const uint32_t term = __ballot_sync(FULL, b < 0x80u);
-      const uint32_t l1 = __ffs(term);
-      const uint32_t rest = l1 ? (term & (~0u << l1)) : 0u;
-      const uint32_t l2end = __ffs(rest);
-      if (!l1 || !l2end) { st = CODAG_ECORRUPT; break; }
-      const uint64_t base = warp_or64(lane < l1 ? shl64(b & 0x7fu, 7u * lane) : 0ull) & m;
-      const uint64_t ud = warp_or64((lane >= l1 && lane < l2end) ? shl64(b & 0x7fu, 7u * (lane - l1)) : 0ull);
+      const uint32_t fbw = v2_width(enc);
+      uint32_t l1, l2;
+      uint64_t ub, ud;
+      if (!read_uvarint(in, pos + 2, end, l1, ub) || !read_uvarint(in, pos + 2 + l1, end, l2, ud)) {
+        st = CODAG_ECORRUPT;
+        break;
+      }
+      const uint64_t base = ub & M;
       const int64_t sd = static_cast<int64_t>(ud);
-      const uint64_t bd = static_cast<uint64_t>((sd >> 1) ^ -(sd & 1)) & m;  // arithmetic shift
+      const uint64_t bd = static_cast<uint64_t>((sd >> 1) ^ -(sd & 1)) & M;  // arithmetic shift (decoder_new.h:990)
       const uint32_t nd = (len8 - 2u) & 0xffu;                              // "len -= 2" on a uint8_t
-      const uint32_t data = pos + 2u + l2end;
-      const uint32_t total = (data - pos) + (enc ? (nd * fbw + 7u) / 8u : 0u);
-      const uint32_t cnt = nd + 2u;
+      const uint32_t data = pos + 2u + l1 + l2;
+      cnt = nd + 2u;
+      total = (data - pos) + (enc ? (nd * fbw + 7u) / 8u : 0u);
       if (pos + total > end || n + cnt > cap) { st = CODAG_ECORRUPT; break; }
-      st = in.ensure(pos + total);
+      st = in.advance(pos, pos + total);
       if (st) break;
       if (enc == 0) {
-        for (uint32_t t = lane; t < cnt; t += 32) out.put(n + t, (base + static_cast<uint64_t>(t) * bd) & m, e);
+        uint64_t v = base + static_cast<uint64_t>(lane) * bd;
+        const uint64_t step = 32ull * bd;
+        for (uint32_t t = lane; t < cnt; t += 32, v += step) put_elem<E>(out, n + t, v & M);
       } else {
         const bool plus = bd != 0;  // multiplier = base_delta > 0 ? 1 : -1 on the unsigned type
-        const uint64_t v1 = (base + bd) & m;
-        if (lane == 0) out.put(n, base, e);
-        if (lane == 1) out.put(n + 1, v1, e);
+        const uint64_t v1 = (base + bd) & M;
+        if (lane == 0) put_elem<E>(out, n, base);
+        if (lane == 1) put_elem<E>(out, n + 1, v1);
         uint64_t carry = v1;
         const uint32_t bit0 = data * 8u;
         for (uint32_t k0 = 0; k0 < nd; k0 += 32) {
           const uint32_t k = k0 + lane;
-          const uint64_t d = k < nd ? (in.bits_be(bit0 + k * fbw, fbw) & m) : 0ull;
+          const uint64_t d = k < nd ? (in.msb_bits64(bit0 + k * fbw, fbw) & M) : 0ull;
           const uint64_t s = warp_scan_add64(d, lane);
-          const uint64_t v = (plus ? carry + s : carry - s) & m;
-          if (k < nd) out.put(n + 2 + k, v, e);
+          const uint64_t v = (plus ? carry + s : carry - s) & M;
+          if (k < nd) put_elem<E>(out, n + 2 + k, v);
           carry = shfl64(v, 31);
         }
       }
-      n += cnt;
-      pos += total;
     } else {  // PATCHED_BASE (decoder_new.h:1092-1183)
-      const uint32_t fbw = kV2WidthDecode[(first >> 1) & 0x1fu];
+      const uint32_t fbw = v2_width((first >> 1) & 0x1fu);
       const uint32_t third = static_cast<uint32_t>(hdr >> 40) & 0xffu;
       const uint32_t fourth = static_cast<uint32_t>(hdr >> 32) & 0xffu;
       const uint32_t bw = ((third >> 5) & 7u) + 1u;
-      const uint32_t pw = kV2WidthDecode[third & 0x1fu];
+      const uint32_t pw = v2_width(third & 0x1fu);
       const uint32_t pgw = ((fourth >> 5) & 7u) + 1u;
       const uint32_t pll = fourth & 0x1fu;
       if (pw + pgw > 64u) { st = CODAG_ECORRUPT; break; }
-      const uint32_t cfb = kV2Closest[pw + pgw];
+      const uint32_t cfb = v2_closest(pw + pgw);
       const uint32_t vals = pos + 4u + bw;
       const uint32_t patches = vals + (len8 * fbw + 7u) / 8u;
-      const uint32_t total = (patches - pos) + (pll * cfb + 7u) / 8u;
-      if (pos + total > end || n + len8 > cap) { st = CODAG_ECORRUPT; break; }
-      st = in.ensure(pos + total);
+      cnt = len8;
+      total = (patches - pos) + (pll * cfb + 7u) / 8u;
+      if (pos + total > end || n + cnt > cap) { st = CODAG_ECORRUPT; break; }
+      st = in.advance(pos, pos + total);
       if (st) break;
       const uint64_t base = in.peek_be64(pos + 4) >> (64u - 8u * bw);
-      for (uint32_t j = lane; j < len8; j += 32)
-        out.put(n + j, (in.bits_be(vals * 8u + j * fbw, fbw) + base) & m, e);
-      __syncwarp();
+      if (fbw <= 32) {
+        for (uint32_t j = lane; j < cnt; j += 32)
+          put_elem<E>(out, n + j, (in.msb_bits32(vals * 8u + j * fbw, fbw) + base) & M);
+      } else {
+        for (uint32_t j = lane; j < cnt; j += 32)
+          put_elem<E>(out, n + j, (in.msb_bits64(vals * 8u + j * fbw, fbw) + base) & M);
+      }
       if (pll) {
         // the reference masks patches with a 32-bit mask (decoder_new.h:1103)
         const uint64_t pmask = pw >= 32 ? 0xffffffffull : ((1ull << pw) - 1ull);
-        uint64_t ent = 0, gap = 0, patch = 0;
+        uint64_t patch = 0;
+        uint32_t gap = 0;
         if (lane < pll) {
-          ent = in.bits_be(patches * 8u + lane * cfb, cfb);
-          gap = shr64(ent, pw);
-          patch = shl64((ent & pmask) & m, fbw) & m;
+          const uint64_t ent = in.msb_bits64(patches * 8u + lane * cfb, cfb);
+          gap = static_cast<uint32_t>(shr64(ent, pw));
+          patch = shl64((ent & pmask) & M, fbw) & M;
         }
-        const uint64_t off = warp_scan_add64(gap, lane);
-        const bool bad = __any_sync(FULL, lane < pll && off >= len8);
-        if (bad) { st = CODAG_ECORRUPT; break; }
-        // OR together the patches of a group of equal offsets into its first lane
-        uint64_t acc = patch;
+        uint32_t off = gap;  // inclusive scan of the gaps (each below 2^8)
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
-          const uint64_t o = shfl_down64(acc, d);
-          const uint64_t ooff = shfl_down64(off, d);
-          if (lane + d < pll && ooff == off) acc |= o;
+          const uint32_t o = __shfl_up_sync(FULL, off, d);
+          if (lane >= static_cast<uint32_t>(d)) off += o;
         }
-        const uint64_t prev_off = shfl_up64(off, 1);
-        const bool head = lane < pll && (lane == 0 || prev_off != off);
-        if (head) {
-          const uint64_t idx = n + off;
-          const uint64_t v = out.get(idx, e);
-          out.put(idx, ((((v - base) & m) | acc) + base) & m, e);
+        if (__any_sync(FULL, lane < pll && off >= len8)) { st = CODAG_ECORRUPT; break; }
+        const uint32_t prev = __shfl_up_sync(FULL, off, 1);
+        if (__any_sync(FULL, lane > 0 && lane < pll && prev == off)) {
+          // several patches on one value: OR the group into its first lane
+#pragma unroll
+          for (int d = 1; d < 32; d <<= 1) {
+            const uint64_t o = shfl_down64(patch, d);
+            const uint32_t ooff = __shfl_down_sync(FULL, off, d);
+            if (lane + d < pll && ooff == off) patch |= o;
+          }
+        }
+        __syncwarp();
+        if (lane < pll && (lane == 0 || prev != off)) {
+          const uint64_t v = get_elem<E>(out, n + off);
+          put_elem<E>(out, n + off, ((((v - base) & M) | patch) + base) & M);
         }
       }
-      n += len8;
-      pos += total;
     }
+    n += cnt;
+    pos += total;
     __syncwarp();
-    out.flush_to(n * static_cast<uint32_t>(e));
+    out.flush_to(static_cast<uint64_t>(n) * E);
   }
   if (!in.drain() && st == CODAG_OK) st = CODAG_ETIMEOUT;
-  out.finish(n * static_cast<uint32_t>(e));
-  if (st == CODAG_OK && n * static_cast<uint32_t>(e) < out.store) st = CODAG_ECORRUPT;
+  out.finish(static_cast<uint64_t>(n) * E);
+  if (st == CODAG_OK && static_cast<uint64_t>(n) * E < out.store) st = CODAG_ECORRUPT;
   return st;
+}
+
+// Element-width dispatch for callers that know the width only at run time.
+template <int NSLOT, class OUT>
+__device__ __noinline__ int decode_rle_any(int codec, InRing<NSLOT>& in, OUT& out, uint64_t chunk_bytes, int e) {
+  const uint32_t cap = static_cast<uint32_t>(chunk_bytes / static_cast<uint32_t>(e));
+  if (codec == CODAG_CODEC_RLEV1) {
+    switch (e) {
+      case 8: return decode_rlev1_chunk<NSLOT, 8>(in, out, cap);
+      case 4: return decode_rlev1_chunk<NSLOT, 4>(in, out, cap);
+      case 2: return decode_rlev1_chunk<NSLOT, 2>(in, out, cap);
+      default: return decode_rlev1_chunk<NSLOT, 1>(in, out, cap);
+    }
+  }
+  switch (e) {
+    case 8: return decode_rlev2_chunk<NSLOT, 8>(in, out, cap);
+    case 4: return decode_rlev2_chunk<NSLOT, 4>(in, out, cap);
+    case 2: return decode_rlev2_chunk<NSLOT, 2>(in, out, cap);
+    default: return decode_rlev2_chunk<NSLOT, 1>(in, out, cap);
+  }
 }
 
 }  // namespace codag_dev

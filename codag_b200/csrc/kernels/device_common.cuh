@@ -128,6 +128,8 @@ struct InRing {
   uint32_t lo, hi;         // stream bytes are [lo, hi) relative to gbase
   uint32_t nslots;         // slots covering [0, hi)
   uint32_t issued, waited; // slots issued / known complete for this chunk
+  uint32_t ready;          // bytes below `ready` are resident (waited << kSlotLog2)
+  uint32_t release_at;     // read position from which release() can issue another slot
   uint32_t phase;          // expected parity per barrier; persists across chunks
   uint64_t wait_cycles;    // bound of one wait
   uint32_t lane;
@@ -141,6 +143,14 @@ struct InRing {
     nslots = (hi + kSlotBytes - 1) >> kSlotLog2;
     issued = 0;
     waited = 0;
+    ready = 0;
+    release_at = 0;
+  }
+
+  // Cheap per-header bookkeeping: refill behind `pos` and make [.., end) resident.
+  __device__ __forceinline__ int advance(uint32_t pos, uint32_t end) {
+    if (pos >= release_at && !release(pos)) return CODAG_ETIMEOUT;
+    return end <= ready ? CODAG_OK : ensure(end);
   }
 
   // Fill slot s: the 16-byte aligned body by TMA, the unaligned head/tail bytes by lanes.
@@ -194,10 +204,12 @@ struct InRing {
       if (issued >= NSLOT && waited <= issued - NSLOT) {  // previous occupant never waited
         if (!wait_slot(waited)) return false;
         waited++;
+        ready = waited << kSlotLog2;
       }
       issue(issued);
       issued++;
     }
+    release_at = issued >= nslots ? 0xffffffffu : (issued + 1 - NSLOT) << kSlotLog2;
     __syncwarp();
     return true;
   }
@@ -212,6 +224,7 @@ struct InRing {
       if (!wait_slot(waited)) return CODAG_ETIMEOUT;
       waited++;
     }
+    ready = waited << kSlotLog2;
     return CODAG_OK;
   }
 
@@ -241,6 +254,22 @@ struct InRing {
     return sh ? (v >> sh) | (static_cast<uint64_t>(w2) << (64 - sh)) : v;
   }
   __device__ __forceinline__ uint64_t peek_be64(uint32_t p) const { return bswap64(peek_le64(p)); }
+  // big-endian 32-bit word at a 4-byte aligned position
+  __device__ __forceinline__ uint32_t be32(uint32_t p4) const { return __byte_perm(rd32(p4), 0, 0x0123); }
+  // w (1..32) bits at stream bit bitpos, most significant bit first (two aligned loads)
+  __device__ __forceinline__ uint32_t msb_bits32(uint32_t bitpos, uint32_t w) const {
+    const uint32_t a = (bitpos >> 5) << 2;
+    const uint32_t top = __funnelshift_l(be32(a + 4), be32(a), bitpos & 31u);
+    return top >> (32u - w);
+  }
+  // w (1..64) bits at stream bit bitpos, most significant bit first (three aligned loads
+  // cover the 64 bits that start anywhere within the first word)
+  __device__ __forceinline__ uint64_t msb_bits64(uint32_t bitpos, uint32_t w) const {
+    const uint32_t a = (bitpos >> 5) << 2, s = bitpos & 31u;
+    const uint32_t w0 = be32(a), w1 = be32(a + 4), w2 = be32(a + 8);
+    const uint64_t v = (static_cast<uint64_t>(__funnelshift_l(w1, w0, s)) << 32) | __funnelshift_l(w2, w1, s);
+    return v >> (64u - w);
+  }
   // `w` (1..64) bits starting at stream bit `bitpos`, most significant bit first; the field
   // must fit in the 8 bytes at bitpos/8, which holds for every ORC RLE v2 width.
   __device__ __forceinline__ uint64_t bits_be(uint32_t bitpos, uint32_t w) const {
