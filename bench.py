@@ -207,16 +207,20 @@ def run_ours(args, rank: int, world: int, local: int):
     d_out = torch.empty(n * CH, dtype=torch.uint8, device=dev)
     d_st = torch.zeros(n, dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream()
+    # two-pass RLE scratch (resident); --rle-passes 1 decodes in a single pass without it
+    d_ws = api.workspace(codec, n, dev) if codec != 2 and args.rle_passes == 2 else None
 
     def launch(comp=d_comp, off=d_off, ln=d_len, out=d_out, obytes=None):
         if codec == 0:
-            api.decompress_rlev1(comp, off, ln, CH, e, out, obytes, d_st, stream)
+            api.decompress_rlev1(comp, off, ln, CH, e, out, obytes, d_st, stream, ws=d_ws)
         elif codec == 1:
-            api.decompress_rlev2(comp, off, ln, CH, e, out, obytes, d_st, stream)
+            api.decompress_rlev2(comp, off, ln, CH, e, out, obytes, d_st, stream, ws=d_ws)
         else:
             api.decompress_deflate(comp, off, CH, out, 2, obytes, d_st, stream)
 
-    if args.autotune:
+    if args.tune:
+        nat.set_tune(codec, *[int(x) for x in args.tune.split(",")])
+    elif args.autotune:
         from codag_b200 import tuning
         best, res = tuning.autotune(codec, launch, use_cache=args.autotune == "cached", verbose=rank == 0)
     for _ in range(max(args.warmup, 3)):
@@ -313,6 +317,8 @@ def run_ours(args, rank: int, world: int, local: int):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
                      "kernel": KERNEL_NAMES[codec], "alg_bytes_per_launch": alg_bytes,
+                     "note": ("launch = header walk + expansion kernels of one call" if codec != 2 and args.rle_passes == 2
+                              else "one kernel"),
                      "launch_ms": round(per_launch * 1e3, 4)},
         "cpu_baseline": cpu,
         "clocks": clk,
@@ -329,6 +335,9 @@ def main():
     ap.add_argument("--workload", default="rlev2", choices=sorted(WORKLOADS) + ["batched"])
     ap.add_argument("--autotune", default="cached", choices=["cached", "search", ""],
                     help="pick the launch shape with the autotuner (cached result or a fresh search)")
+    ap.add_argument("--rle-passes", type=int, default=1, choices=[1, 2],
+                    help="RLE: 2 = header walk + expansion (with workspace), 1 = single pass")
+    ap.add_argument("--tune", default="", help="explicit launch shape warps_per_cta,ring_slots,lut_bits")
     ap.add_argument("--n-values", type=int, default=None,
                     help="override the workload's element count (profiling cases; not a bench line)")
     args = ap.parse_args()

@@ -49,24 +49,44 @@ def _status_error(where: str, status: torch.Tensor) -> None:
 
 
 # --- device calls (C ABI, caller-owned device buffers) ----------------------------------------
+def workspace(codec: int, n_chunks: int, device="cuda") -> torch.Tensor:
+    """A device workspace for the two-pass RLE decode of n_chunks chunks."""
+    nbytes = int(native.lib().codag_workspace_bytes(codec, n_chunks))
+    return torch.empty(max(nbytes, 256), dtype=torch.uint8, device=device)
+
+
+AUTO_WORKSPACE = object()  # ws=AUTO_WORKSPACE: allocate a workspace for this call (two-pass decode)
+
+
+def _ws(codec, n, ws):
+    if ws is AUTO_WORKSPACE:
+        ws = workspace(codec, n)
+    return (_dptr(ws), ws.numel()) if ws is not None else (None, 0)
+
+
 def decompress_rlev1(comp: torch.Tensor, blk_off: torch.Tensor, col_len: torch.Tensor, chunk_bytes: int,
                      elem_bytes: int, out: torch.Tensor, out_bytes: int | None = None,
-                     status: torch.Tensor | None = None, stream=None) -> None:
-    """codag_decompress_rlev1: comp is the stream base (blob+8), blk_off/col_len have n entries."""
+                     status: torch.Tensor | None = None, stream=None, ws=None) -> None:
+    """codag_decompress_rlev1: comp is the stream base (blob+8), blk_off/col_len have n entries.
+    ws: None (default) decodes each chunk in one pass; a workspace tensor (see workspace()) or
+    AUTO_WORKSPACE selects the two-pass decode (header walk, then descriptor-driven expansion)."""
     n = col_len.numel()
+    wp, wb = _ws(native.RLEV1, n, ws)
     check("codag_decompress_rlev1", native.lib().codag_decompress_rlev1(
         _dptr(comp), comp.numel(), _dptr(blk_off), _dptr(col_len), n, chunk_bytes, elem_bytes, _dptr(out),
-        out.numel() if out_bytes is None else out_bytes, _dptr(status), _stream(stream)))
+        out.numel() if out_bytes is None else out_bytes, _dptr(status), wp, wb, _stream(stream)))
 
 
 def decompress_rlev2(comp: torch.Tensor, blk_off: torch.Tensor, col_len: torch.Tensor, chunk_bytes: int,
                      elem_bytes: int, out: torch.Tensor, out_bytes: int | None = None,
-                     status: torch.Tensor | None = None, stream=None) -> None:
-    """codag_decompress_rlev2: blk_off/col_len have n entries (the size entry is not passed)."""
+                     status: torch.Tensor | None = None, stream=None, ws=None) -> None:
+    """codag_decompress_rlev2: blk_off/col_len have n entries (the size entry is not passed).
+    ws as for decompress_rlev1."""
     n = col_len.numel()
+    wp, wb = _ws(native.RLEV2, n, ws)
     check("codag_decompress_rlev2", native.lib().codag_decompress_rlev2(
         _dptr(comp), comp.numel(), _dptr(blk_off), _dptr(col_len), n, chunk_bytes, elem_bytes, _dptr(out),
-        out.numel() if out_bytes is None else out_bytes, _dptr(status), _stream(stream)))
+        out.numel() if out_bytes is None else out_bytes, _dptr(status), wp, wb, _stream(stream)))
 
 
 def decompress_deflate(comp: torch.Tensor, blk_off: torch.Tensor, chunk_bytes: int, out: torch.Tensor,

@@ -15,6 +15,7 @@
 
 #include "decode_deflate.cuh"
 #include "decode_rle.cuh"
+#include "walk_rle.cuh"
 
 using namespace codag_dev;
 
@@ -60,13 +61,33 @@ __device__ __forceinline__ bool stream_in_bounds(uint64_t off, uint64_t len, uin
 // ---------------------------------------------------------------------------------------
 // plain kernels: chunk = blockIdx.x * warps + warp
 // ---------------------------------------------------------------------------------------
+// header walk, one thread per chunk; descriptors and counts go to the workspace
+template <int CODEC>
+__global__ void __launch_bounds__(128) k_rle_walk(const uint8_t* __restrict__ comp, uint64_t comp_bytes,
+                                                  const uint64_t* __restrict__ blk_off,
+                                                  const uint64_t* __restrict__ col_len, uint64_t n_chunks,
+                                                  uint32_t cap, uint32_t* __restrict__ counts,
+                                                  RleDesc* __restrict__ descs) {
+  const uint64_t chunk = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (chunk >= n_chunks) return;
+  const uint64_t off = blk_off[chunk], len = col_len[chunk];
+  uint32_t k = kWalkFallback;
+  if (stream_in_bounds(off, len, comp_bytes)) {
+    const GStream g{comp + off, static_cast<uint32_t>(len), comp, comp + comp_bytes};
+    RleDesc* d = descs + chunk * kDescPerChunk;
+    k = CODEC == CODAG_CODEC_RLEV1 ? walk_rlev1(g, cap, d) : walk_rlev2(g, cap, d);
+  }
+  counts[chunk] = k;
+}
+
 template <int NSLOT, int CODEC, int E>
 __global__ void __launch_bounds__(256) k_rle_plain(const uint8_t* __restrict__ comp, uint64_t comp_bytes,
                                                    const uint64_t* __restrict__ blk_off,
                                                    const uint64_t* __restrict__ col_len, uint64_t n_chunks,
                                                    uint64_t chunk_bytes, uint8_t* __restrict__ out,
                                                    uint64_t out_bytes, int32_t* __restrict__ status,
-                                                   uint64_t wait_cycles) {
+                                                   uint64_t wait_cycles, const uint32_t* __restrict__ counts,
+                                                   const RleDesc* __restrict__ descs) {
   extern __shared__ __align__(128) uint8_t smem[];
   using L = RleLayout<NSLOT>;
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
@@ -75,12 +96,14 @@ __global__ void __launch_bounds__(256) k_rle_plain(const uint8_t* __restrict__ c
   uint8_t* base = smem + warp * L::kPerWarp;
   InRing<NSLOT> in;
   in.buf = base + L::kIn;
+  in.sbuf = smem_u32(in.buf);
   in.bar = reinterpret_cast<uint64_t*>(base + L::kBar);
   in.phase = 0;
   in.wait_cycles = wait_cycles;
   in.lane = lane;
   RleOut o;
   o.buf = base + L::kOut;
+  o.sbuf = smem_u32(o.buf);
   o.lane = lane;
   init_ring_barriers<NSLOT>(in.bar, lane);
 
@@ -93,7 +116,13 @@ __global__ void __launch_bounds__(256) k_rle_plain(const uint8_t* __restrict__ c
     in.begin(comp + off, static_cast<uint32_t>(len));
     o.begin(out + cbase, store_bytes(cbase, chunk_bytes, out_bytes));
     const uint32_t cap = static_cast<uint32_t>(chunk_bytes / E);
-    st = CODEC == CODAG_CODEC_RLEV1 ? decode_rlev1_chunk<NSLOT, E>(in, o, cap) : decode_rlev2_chunk<NSLOT, E>(in, o, cap);
+    const uint32_t nd = counts ? counts[chunk] : kWalkFallback;
+    if (nd != kWalkFallback) {
+      const RleDesc* d = descs + chunk * kDescPerChunk;
+      st = CODEC == CODAG_CODEC_RLEV1 ? expand_rlev1<NSLOT, E>(in, o, d, nd) : expand_rlev2<NSLOT, E>(in, o, d, nd);
+    } else {
+      st = CODEC == CODAG_CODEC_RLEV1 ? decode_rlev1_chunk<NSLOT, E>(in, o, cap) : decode_rlev2_chunk<NSLOT, E>(in, o, cap);
+    }
   }
   if (status && lane == 0) status[chunk] = st;
 }
@@ -112,12 +141,14 @@ __global__ void __launch_bounds__(256) k_inflate_plain(const uint8_t* __restrict
   uint8_t* base = smem + warp * L::kPerWarp;
   InRing<NSLOT> in;
   in.buf = base + L::kIn;
+  in.sbuf = smem_u32(in.buf);
   in.bar = reinterpret_cast<uint64_t*>(base + L::kBar);
   in.phase = 0;
   in.wait_cycles = wait_cycles;
   in.lane = lane;
   InflateOut o;
   o.buf = base + L::kOut;
+  o.sbuf = smem_u32(o.buf);
   o.lane = lane;
   auto& sc = *reinterpret_cast<InflateScratch<LB>*>(base + L::kScratch);
   init_ring_barriers<NSLOT>(in.bar, lane);
@@ -150,12 +181,14 @@ __global__ void __launch_bounds__(256) k_batch(const codag_chunk_desc* __restric
   uint8_t* base = smem + warp * L::kPerWarp;
   InRing<NSLOT> in;
   in.buf = base + L::kIn;
+  in.sbuf = smem_u32(in.buf);
   in.bar = reinterpret_cast<uint64_t*>(base + L::kBar);
   in.phase = 0;
   in.wait_cycles = wait_cycles;
   in.lane = lane;
   InflateOut o;
   o.buf = base + L::kOut;
+  o.sbuf = smem_u32(o.buf);
   o.lane = lane;
   auto& sc = *reinterpret_cast<InflateScratch<LB>*>(base + L::kScratch);
   init_ring_barriers<NSLOT>(in.bar, lane);
@@ -193,6 +226,7 @@ __global__ void k_selftest_timeout(int32_t* status, uint64_t wait_cycles) {
   const uint32_t lane = threadIdx.x & 31u;
   InRing<1> in;
   in.buf = buf;
+  in.sbuf = smem_u32(buf);
   in.bar = bar;
   in.phase = 0;
   in.wait_cycles = wait_cycles;
@@ -235,31 +269,43 @@ codag_status finish_launch() {
   return err == cudaSuccess ? CODAG_OK : CODAG_ECUDA;
 }
 
+// workspace of the two-pass RLE path: per-chunk descriptor counts, then descriptor tables
+uint64_t rle_ws_counts_bytes(uint64_t n) { return (n * 4 + 255) / 256 * 256; }
+uint64_t rle_ws_bytes(uint64_t n) { return rle_ws_counts_bytes(n) + n * kDescPerChunk * sizeof(RleDesc); }
+
 template <int NSLOT, int CODEC, int E>
 codag_status launch_rle(const codag_tune& t, const uint8_t* comp, uint64_t comp_bytes, const uint64_t* blk_off,
                         const uint64_t* col_len, uint64_t n, uint64_t chunk_bytes, uint8_t* out, uint64_t out_bytes,
-                        int32_t* status, cudaStream_t s) {
+                        int32_t* status, void* ws, uint64_t ws_bytes, cudaStream_t s) {
   using L = RleLayout<NSLOT>;
   const uint32_t smem = L::kPerWarp * t.warps_per_cta;
   auto kern = k_rle_plain<NSLOT, CODEC, E>;
   if (allow_smem(kern, smem) != cudaSuccess) return CODAG_ECUDA;
   const uint64_t grid = (n + t.warps_per_cta - 1) / t.warps_per_cta;
   if (grid > 0x7fffffffull) return CODAG_EINVAL;
+  uint32_t* counts = nullptr;
+  RleDesc* descs = nullptr;
+  if (ws && ws_bytes >= rle_ws_bytes(n) && (reinterpret_cast<uintptr_t>(ws) & 255) == 0) {
+    counts = static_cast<uint32_t*>(ws);
+    descs = reinterpret_cast<RleDesc*>(static_cast<uint8_t*>(ws) + rle_ws_counts_bytes(n));
+    k_rle_walk<CODEC><<<static_cast<unsigned>((n + 127) / 128), 128, 0, s>>>(
+        comp, comp_bytes, blk_off, col_len, n, static_cast<uint32_t>(chunk_bytes / E), counts, descs);
+  }
   kern<<<static_cast<unsigned>(grid), 32 * t.warps_per_cta, smem, s>>>(comp, comp_bytes, blk_off, col_len, n,
                                                                          chunk_bytes, out, out_bytes, status,
-                                                                         wait_of());
+                                                                         wait_of(), counts, descs);
   return finish_launch();
 }
 
 template <int NSLOT, int CODEC>
 codag_status launch_rle_e(const codag_tune& t, const uint8_t* comp, uint64_t comp_bytes, const uint64_t* blk_off,
                           const uint64_t* col_len, uint64_t n, uint64_t chunk_bytes, int e, uint8_t* out,
-                          uint64_t out_bytes, int32_t* status, cudaStream_t s) {
+                          uint64_t out_bytes, int32_t* status, void* ws, uint64_t wsb, cudaStream_t s) {
   switch (e) {
-    case 8: return launch_rle<NSLOT, CODEC, 8>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, out, out_bytes, status, s);
-    case 4: return launch_rle<NSLOT, CODEC, 4>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, out, out_bytes, status, s);
-    case 2: return launch_rle<NSLOT, CODEC, 2>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, out, out_bytes, status, s);
-    default: return launch_rle<NSLOT, CODEC, 1>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, out, out_bytes, status, s);
+    case 8: return launch_rle<NSLOT, CODEC, 8>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, out, out_bytes, status, ws, wsb, s);
+    case 4: return launch_rle<NSLOT, CODEC, 4>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, out, out_bytes, status, ws, wsb, s);
+    case 2: return launch_rle<NSLOT, CODEC, 2>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, out, out_bytes, status, ws, wsb, s);
+    default: return launch_rle<NSLOT, CODEC, 1>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, out, out_bytes, status, ws, wsb, s);
   }
 }
 
@@ -282,15 +328,15 @@ codag_status launch_inflate(const codag_tune& t, const uint8_t* comp, uint64_t c
 template <int CODEC>
 codag_status dispatch_rle(const uint8_t* comp, uint64_t comp_bytes, const uint64_t* blk_off, const uint64_t* col_len,
                           uint64_t n, uint64_t chunk_bytes, int e, uint8_t* out, uint64_t out_bytes, int32_t* status,
-                          cudaStream_t s) {
+                          void* ws, uint64_t wsb, cudaStream_t s) {
   if (!comp || !blk_off || !col_len || (!out && out_bytes) || !valid_elem(e) || chunk_bytes == 0 ||
       chunk_bytes % static_cast<uint64_t>(e) || chunk_bytes >= (1ull << 31))
     return CODAG_EINVAL;
   if (n == 0) return CODAG_OK;
   const codag_tune t = tune_of(CODEC);
   if (t.ring_slots == 4)
-    return launch_rle_e<4, CODEC>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, e, out, out_bytes, status, s);
-  return launch_rle_e<8, CODEC>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, e, out, out_bytes, status, s);
+    return launch_rle_e<4, CODEC>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, e, out, out_bytes, status, ws, wsb, s);
+  return launch_rle_e<8, CODEC>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, e, out, out_bytes, status, ws, wsb, s);
 }
 
 }  // namespace
@@ -298,20 +344,28 @@ codag_status dispatch_rle(const uint8_t* comp, uint64_t comp_bytes, const uint64
 // ---------------------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------------------
+extern "C" uint64_t codag_workspace_bytes(int codec, uint64_t n_chunks) {
+  return (codec == CODAG_CODEC_RLEV1 || codec == CODAG_CODEC_RLEV2) ? rle_ws_bytes(n_chunks) : 0;
+}
+
 extern "C" codag_status codag_decompress_rlev1(const uint8_t* d_comp, uint64_t comp_bytes, const uint64_t* d_blk_off,
                                                const uint64_t* d_col_len, uint64_t n_chunks, uint64_t chunk_bytes,
                                                int elem_bytes, uint8_t* d_out, uint64_t out_bytes,
-                                               int32_t* d_chunk_status, codag_stream_t stream) {
+                                               int32_t* d_chunk_status, void* d_workspace, uint64_t workspace_bytes,
+                                               codag_stream_t stream) {
   return dispatch_rle<CODAG_CODEC_RLEV1>(d_comp, comp_bytes, d_blk_off, d_col_len, n_chunks, chunk_bytes, elem_bytes,
-                                         d_out, out_bytes, d_chunk_status, reinterpret_cast<cudaStream_t>(stream));
+                                         d_out, out_bytes, d_chunk_status, d_workspace, workspace_bytes,
+                                         reinterpret_cast<cudaStream_t>(stream));
 }
 
 extern "C" codag_status codag_decompress_rlev2(const uint8_t* d_comp, uint64_t comp_bytes, const uint64_t* d_blk_off,
                                                const uint64_t* d_col_len, uint64_t n_chunks, uint64_t chunk_bytes,
                                                int elem_bytes, uint8_t* d_out, uint64_t out_bytes,
-                                               int32_t* d_chunk_status, codag_stream_t stream) {
+                                               int32_t* d_chunk_status, void* d_workspace, uint64_t workspace_bytes,
+                                               codag_stream_t stream) {
   return dispatch_rle<CODAG_CODEC_RLEV2>(d_comp, comp_bytes, d_blk_off, d_col_len, n_chunks, chunk_bytes, elem_bytes,
-                                         d_out, out_bytes, d_chunk_status, reinterpret_cast<cudaStream_t>(stream));
+                                         d_out, out_bytes, d_chunk_status, d_workspace, workspace_bytes,
+                                         reinterpret_cast<cudaStream_t>(stream));
 }
 
 extern "C" codag_status codag_decompress_deflate(const uint8_t* d_comp, uint64_t comp_bytes, const uint64_t* d_blk_off,

@@ -188,9 +188,9 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<
   const HuffTable lit{sc.lit_lut, sc.lit_sorted, sc.lit_cnt, sc.lit_first, sc.lit_index, LB};
   const HuffTable dst{sc.dist_lut, sc.dist_sorted, sc.dist_cnt, sc.dist_first, sc.dist_index, kDistLB};
   const HuffTable cl{sc.dist_lut, sc.dist_sorted, sc.dist_cnt, sc.dist_first, sc.dist_index, kCodeLenLB};
-  constexpr uint32_t kOutMask = OUT::kMask;
+  const uint32_t s_lit = smem_u32(sc.lit_lut), s_dist = smem_u32(sc.dist_lut);
 
-  uint64_t op = 0;  // bytes produced
+  uint32_t op = 0;  // bytes produced (chunks are < 2 GiB)
   int st = CODAG_OK;
   BitReader<NSLOT> br;
   bool fixed_ready = false;
@@ -230,7 +230,7 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<
         if (!in.release(p)) { st = CODAG_ETIMEOUT; break; }
         st = in.ensure(p + piece);
         if (st) break;
-        for (uint32_t t = lane; t < piece; t += 32) out.buf[(op + t) & kOutMask] = static_cast<uint8_t>(in.rd8(p + t));
+        for (uint32_t t = lane; t < piece; t += 32) out.put8(op + t, in.rd8(p + t));
         op += piece;
         p += piece;
         left -= piece;
@@ -281,7 +281,7 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<
       const uint32_t total = hlit + hdist;
       while (idx < total) {
         CODAG_REFILL();
-        const uint32_t e = cl.lut[br.bb & ((1u << kCodeLenLB) - 1u)];
+        const uint32_t e = ld_s32(s_dist + 4u * static_cast<uint32_t>(br.bb & ((1u << kCodeLenLB) - 1u)));
         if (!e) { st = CODAG_ECORRUPT; break; }
         br.drop(e & 15u);
         const uint32_t sym = e >> 16;
@@ -327,7 +327,7 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<
     // symbol loop (zlib.h:712-805)
     for (;;) {
       CODAG_REFILL();
-      uint32_t e = lit.lut[br.bb & ((1u << LB) - 1u)];
+      uint32_t e = ld_s32(s_lit + 4u * static_cast<uint32_t>(br.bb & ((1u << LB) - 1u)));
       if (!e) {
         e = slow_entry(br.bb, lit, kAlphaLitLen);
         if (!e) { st = CODAG_ECORRUPT; break; }
@@ -336,7 +336,7 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<
       br.drop(e & 15u);
       if (kind == kKindLit) {
         if (op >= cap) { st = CODAG_ECORRUPT; break; }
-        if (lane == 0) out.buf[op & kOutMask] = static_cast<uint8_t>(e >> 16);
+        if (lane == 0) out.put8(op, e >> 16);
         op++;
         if (op - out.flushed >= OUT::kFlush) out.flush_to(op);
         continue;
@@ -347,7 +347,7 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<
       const uint32_t len = (e >> 16) + (static_cast<uint32_t>(br.bb) & ((1u << lext) - 1u));
       br.drop(lext);
       CODAG_REFILL();
-      uint32_t d = dst.lut[br.bb & ((1u << kDistLB) - 1u)];
+      uint32_t d = ld_s32(s_dist + 4u * static_cast<uint32_t>(br.bb & ((1u << kDistLB) - 1u)));
       if (!d) {
         d = slow_entry(br.bb, dst, kAlphaDist);
         if (!d) { st = CODAG_ECORRUPT; break; }
@@ -361,12 +361,12 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<
       __syncwarp();
       if (dist + len <= OUT::kBytes) {  // source still in the shared-memory window
         if (dist >= len) {
-          for (uint32_t t = lane; t < len; t += 32) out.buf[(op + t) & kOutMask] = out.buf[(op - dist + t) & kOutMask];
+          for (uint32_t t = lane; t < len; t += 32) out.put8(op + t, out.get8(op - dist + t));
         } else {
           uint32_t r = lane % dist;
           const uint32_t step = 32u % dist;
           for (uint32_t t = lane; t < len; t += 32) {
-            out.buf[(op + t) & kOutMask] = out.buf[(op - dist + r) & kOutMask];
+            out.put8(op + t, out.get8(op - dist + r));
             r += step;
             if (r >= dist) r -= dist;
           }
@@ -377,7 +377,7 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<
         const uint32_t step = dist >= len ? 32u : 32u % dist;
         for (uint32_t t = lane; t < len; t += 32) {
           const uint64_t s = src0 + r;
-          out.buf[(op + t) & kOutMask] = s < out.store ? out.gdst[s] : 0;  // unstored bytes are never stored either
+          out.put8(op + t, s < out.store ? out.gdst[s] : 0u);  // unstored bytes are never stored either
           r += step;
           if (dist < len && r >= dist) r -= dist;
         }

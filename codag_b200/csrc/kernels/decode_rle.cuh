@@ -2,22 +2,25 @@
 //
 // CODAG decodes these with one lane walking the stream byte by byte while the other lanes
 // idle or store the same addresses (include/rlev1/decoder.h:588-798,
-// include/rlev2/decoder_new.h:909-1187).  Here the header walk stays sequential (each
-// header's size depends on its contents) but is kept to a few dozen warp instructions per
-// header, and everything inside a header is lane-parallel:
-//   - headers are read with one 8-byte big-endian peek; LEB128 varints are decoded in
-//     registers by compacting the 7-bit groups of an 8- or 16-byte window;
-//   - RLE v1 literal groups are scanned 128 bytes per step, 4 bytes per lane: one ballot per
-//     byte lane finds the varint ends, and the lane holding an end decodes that varint;
-//   - RLE v1 runs and RLE v2 SHORT_REPEAT/fixed-step DELTA values are produced one per lane;
-//   - RLE v2 DIRECT/PATCHED_BASE values are unpacked one per lane by direct bit addressing
-//     (two or three aligned shared-memory words and a funnel shift);
-//   - RLE v2 packed DELTA deltas are accumulated with a warp scan;
-//   - PATCHED_BASE patch offsets are prefix-summed across the patch lanes and applied by
-//     those lanes (a group of patches hitting one value is OR-combined first).
-// Decoded values go to the shared-memory output ring (OutRing) and leave it as 16-byte
-// stores.  Element arithmetic is modulo 2^(8*E), keeping the reference's quirks (see
-// oracle/oracle.c for the list).
+// include/rlev2/decoder_new.h:909-1187).  Here each chunk is decoded in two passes when a
+// workspace is available (walk_rle.cuh):
+//   1. a header walk, one THREAD per chunk (so one warp instruction advances 32 chunks),
+//      writes a 32-byte descriptor per header;
+//   2. one WARP per chunk expands the headers: descriptors arrive 32 at a time with one
+//      coalesced load, and each header's values are produced lane-parallel.
+// Without a workspace the same warp parses the headers itself (decode_rlev*_chunk).
+// Lane-parallel value expansion, shared by both paths:
+//   - RLE v1 runs, RLE v2 SHORT_REPEAT and fixed-step DELTA: one arithmetic value per lane;
+//   - RLE v1 literal groups: 128 stream bytes per step, 4 bytes per lane; one ballot per byte
+//     lane finds the varint ends and the lane holding an end decodes that varint in registers
+//     (7-bit groups compacted with shifts and masks);
+//   - RLE v2 DIRECT/PATCHED_BASE: one value per lane by direct bit addressing (two or three
+//     aligned shared-memory words and a funnel shift);
+//   - RLE v2 packed DELTA: deltas unpacked per lane and accumulated with a warp scan;
+//   - PATCHED_BASE patches: gaps prefix-summed across the patch lanes, patches applied by
+//     those lanes (a group hitting one value is OR-combined first).
+// Values go to the shared-memory output ring (OutRing) and leave it as 16-byte stores.
+// Element arithmetic is modulo 2^(8*E), keeping the reference's quirks (oracle/oracle.c).
 #pragma once
 #include "device_common.cuh"
 
@@ -41,27 +44,33 @@ __device__ __forceinline__ constexpr uint64_t emask() {
 
 template <int E, class OUT>
 __device__ __forceinline__ void put_elem(OUT& o, uint32_t idx, uint64_t v) {
-  using T = typename ElemType<E>::T;
-  *reinterpret_cast<T*>(o.buf + ((idx * static_cast<uint32_t>(E)) & OUT::kMask)) = static_cast<T>(v);
+  const uint32_t a = o.sbuf + ((idx * static_cast<uint32_t>(E)) & OUT::kMask);
+  if constexpr (E == 8) st_s64(a, v);
+  else if constexpr (E == 4) st_s32(a, static_cast<uint32_t>(v));
+  else if constexpr (E == 2) st_s16(a, static_cast<uint32_t>(v));
+  else st_s8(a, static_cast<uint32_t>(v));
 }
 
 template <int E, class OUT>
 __device__ __forceinline__ uint64_t get_elem(const OUT& o, uint32_t idx) {
-  using T = typename ElemType<E>::T;
-  return *reinterpret_cast<const T*>(o.buf + ((idx * static_cast<uint32_t>(E)) & OUT::kMask));
+  const uint32_t a = o.sbuf + ((idx * static_cast<uint32_t>(E)) & OUT::kMask);
+  if constexpr (E == 8) return ld_s64(a);
+  else if constexpr (E == 4) return ld_s32(a);
+  else if constexpr (E == 2) return ld_s16(a);
+  else return ld_s8(a);
 }
 
 // bit width of a 5-bit width code (include/rlev2/utils.h:28)
-__device__ __forceinline__ uint32_t v2_width(uint32_t c) {
+__host__ __device__ __forceinline__ uint32_t v2_width(uint32_t c) {
   return c < 24 ? c + 1 : (c < 28 ? 2 * c - 22 : 8 * c - 184);
 }
 // smallest representable width >= b, for b in 0..64 (utils.h:42-48)
-__device__ __forceinline__ uint32_t v2_closest(uint32_t b) {
+__host__ __device__ __forceinline__ uint32_t v2_closest(uint32_t b) {
   return b <= 24 ? (b ? b : 1u) : (b <= 32 ? (b + 1) & ~1u : (b + 7) & ~7u);
 }
 
 // LEB128 payload of the first `len` bytes of a little-endian window (len 1..8)
-__device__ __forceinline__ uint64_t leb_compact(uint64_t x, uint32_t len) {
+__host__ __device__ __forceinline__ uint64_t leb_compact(uint64_t x, uint32_t len) {
   if (len < 8) x &= (1ull << (8 * len)) - 1ull;
   x &= 0x7F7F7F7F7F7F7F7Full;
   x = (x & 0x007F007F007F007Full) | ((x >> 1) & 0x3F803F803F803F80ull);
@@ -69,11 +78,32 @@ __device__ __forceinline__ uint64_t leb_compact(uint64_t x, uint32_t len) {
   x = (x & 0x000000000FFFFFFFull) | ((x >> 4) & 0x00FFFFFFF0000000ull);
   return x;
 }
+// the same for len 1..4 in 32-bit arithmetic
+__device__ __forceinline__ uint32_t leb_compact32(uint32_t x, uint32_t len) {
+  if (len < 4) x &= (1u << (8 * len)) - 1u;
+  x &= 0x7F7F7F7Fu;
+  x = (x & 0x007F007Fu) | ((x >> 1) & 0x3F803F80u);
+  return (x & 0x00003FFFu) | ((x >> 2) & 0x0FFFC000u);
+}
 // value of a LEB128 varint of `len` bytes whose first 16 bytes are lo8, hi8; bytes past
 // the 10th only feed bits above 63 and vanish, as with the reference's clamped shifts
-__device__ __forceinline__ uint64_t leb_value(uint64_t lo8, uint64_t hi8, uint32_t len) {
+__host__ __device__ __forceinline__ uint64_t leb_value(uint64_t lo8, uint64_t hi8, uint32_t len) {
   if (len <= 8) return leb_compact(lo8, len);
   return leb_compact(lo8, 8) | (leb_compact(hi8, len - 8 < 8 ? len - 8 : 8) << 56);
+}
+__host__ __device__ __forceinline__ uint32_t ctz64(uint64_t t) {
+#ifdef __CUDA_ARCH__
+  return static_cast<uint32_t>(__ffsll(static_cast<long long>(t)) - 1);
+#else
+  return static_cast<uint32_t>(__builtin_ctzll(t));
+#endif
+}
+// length (1..16) of the varint that starts a 16-byte window, or 0 if it is longer
+__host__ __device__ __forceinline__ uint32_t leb_len(uint64_t lo8, uint64_t hi8) {
+  uint64_t t = ~lo8 & 0x8080808080808080ull;
+  if (t) return (ctz64(t) >> 3) + 1;
+  t = ~hi8 & 0x8080808080808080ull;
+  return t ? (ctz64(t) >> 3) + 9 : 0u;
 }
 
 // Reads the unsigned varint at `p` (all lanes, same data); false if it is truncated or
@@ -83,120 +113,236 @@ __device__ __forceinline__ bool read_uvarint(InRing<NSLOT>& in, uint32_t p, uint
                                              uint64_t& val) {
   if (p + 20 > in.ready && in.ensure(min(p + 20, end))) return false;
   const uint64_t lo8 = in.peek_le64(p);
-  uint64_t t = ~lo8 & 0x8080808080808080ull;
+  const uint64_t t = ~lo8 & 0x8080808080808080ull;
   if (t) {
     len = (static_cast<uint32_t>(__ffsll(t)) >> 3);
     val = leb_compact(lo8, len);
   } else {
     const uint64_t hi8 = in.peek_le64(p + 8);
-    t = ~hi8 & 0x8080808080808080ull;
-    if (t) {
-      len = 8 + (static_cast<uint32_t>(__ffsll(t)) >> 3);
-      val = leb_value(lo8, hi8, len);
-    } else {  // longer than 16 bytes: only the first 16 carry bits; find the end
+    len = leb_len(lo8, hi8);
+    if (!len) {  // longer than 16 bytes: only the first 16 carry bits; find the end
       uint32_t q = p + 16;
       const uint32_t lim = min(end, p + 1024);
       if (in.ensure(lim)) return false;
       while (q < lim && in.rd8(q) >= 0x80u) q++;
       if (q >= lim) return false;
       len = q - p + 1;
-      val = leb_value(lo8, hi8, len);
     }
+    val = leb_value(lo8, hi8, len);
   }
   return p + len <= end;
 }
 
 // ---------------------------------------------------------------------------------------
-// ORC RLE v1
+// per-header value expansion (warp-cooperative; all lanes call with identical arguments)
 // ---------------------------------------------------------------------------------------
-// Decodes one chunk of `cap` elements.  Loops while fewer than cap elements were produced,
-// as the reference does (decoder.h:669).
+// store v (E bytes) at shared address a
+template <int E>
+__device__ __forceinline__ void st_elem(uint32_t a, uint64_t v) {
+  if constexpr (E == 8) st_s64(a, v);
+  else if constexpr (E == 4) st_s32(a, static_cast<uint32_t>(v));
+  else if constexpr (E == 2) st_s16(a, static_cast<uint32_t>(v));
+  else st_s8(a, static_cast<uint32_t>(v));
+}
+
+// value i = v + i*step, i < cnt
+template <int E, class OUT>
+__device__ __forceinline__ void body_fill(OUT& out, uint32_t n, uint32_t cnt, uint64_t v, uint64_t step, uint32_t lane) {
+  if (lane >= cnt) return;
+  uint64_t x = v + static_cast<uint64_t>(lane) * step;
+  const uint64_t s32 = step << 5;
+  uint32_t oa = (n + lane) * E;
+  const uint32_t base = out.sbuf;
+  for (uint32_t i = lane; i < cnt; i += 32, x += s32, oa += 32 * E) st_elem<E>(base + (oa & OUT::kMask), x);
+}
+
+// value i = (fbw-bit field i at bit0, most significant bit first) + add, i < cnt
+template <int NSLOT, int E, class OUT>
+__device__ __forceinline__ void body_unpack(const InRing<NSLOT>& in, OUT& out, uint32_t n, uint32_t cnt, uint32_t bit0,
+                                            uint32_t fbw, uint64_t add, uint32_t lane) {
+  if (lane >= cnt) return;
+  constexpr uint32_t IM = InRing<NSLOT>::kMask;
+  const uint32_t ib = in.sbuf, ob = out.sbuf;
+  uint32_t bp = bit0 + lane * fbw;
+  const uint32_t bstep = fbw << 5;
+  uint32_t oa = (n + lane) * E;
+  if (fbw <= 32) {
+    const uint32_t rs = 32u - fbw;
+    for (uint32_t j = lane; j < cnt; j += 32, bp += bstep, oa += 32 * E) {
+      const uint32_t wa = (bp >> 3) & ~3u;
+      const uint32_t w0 = __byte_perm(ld_s32(ib + (wa & IM)), 0, 0x0123);
+      const uint32_t w1 = __byte_perm(ld_s32(ib + ((wa + 4) & IM)), 0, 0x0123);
+      const uint32_t v = __funnelshift_l(w1, w0, bp & 31u) >> rs;
+      st_elem<E>(ob + (oa & OUT::kMask), static_cast<uint64_t>(v) + add);
+    }
+  } else {
+    const uint32_t rs = 64u - fbw;
+    for (uint32_t j = lane; j < cnt; j += 32, bp += bstep, oa += 32 * E) {
+      const uint32_t wa = (bp >> 3) & ~3u, s = bp & 31u;
+      const uint32_t w0 = __byte_perm(ld_s32(ib + (wa & IM)), 0, 0x0123);
+      const uint32_t w1 = __byte_perm(ld_s32(ib + ((wa + 4) & IM)), 0, 0x0123);
+      const uint32_t w2 = __byte_perm(ld_s32(ib + ((wa + 8) & IM)), 0, 0x0123);
+      const uint64_t v = ((static_cast<uint64_t>(__funnelshift_l(w1, w0, s)) << 32) | __funnelshift_l(w2, w1, s)) >> rs;
+      st_elem<E>(ob + (oa & OUT::kMask), v + add);
+    }
+  }
+}
+
+// packed DELTA: values base, base+bd, then += (or -=) each of nd packed deltas
+template <int NSLOT, int E, class OUT>
+__device__ __forceinline__ void body_delta_packed(const InRing<NSLOT>& in, OUT& out, uint32_t n, uint32_t nd,
+                                                  uint32_t fbw, uint64_t base, uint64_t bd, uint32_t bit0,
+                                                  uint32_t lane) {
+  constexpr uint64_t M = emask<E>();
+  const bool plus = bd != 0;  // multiplier = base_delta > 0 ? 1 : -1 on the unsigned type
+  const uint64_t v1 = (base + bd) & M;
+  if (lane == 0) put_elem<E>(out, n, base);
+  if (lane == 1) put_elem<E>(out, n + 1, v1);
+  uint64_t carry = v1;
+  for (uint32_t k0 = 0; k0 < nd; k0 += 32) {
+    const uint32_t k = k0 + lane;
+    const uint64_t d = k < nd ? (in.msb_bits64(bit0 + k * fbw, fbw) & M) : 0ull;
+    const uint64_t s = warp_scan_add64(d, lane);
+    const uint64_t v = (plus ? carry + s : carry - s) & M;
+    if (k < nd) put_elem<E>(out, n + 2 + k, v);
+    carry = shfl64(v, 31);
+  }
+}
+
+// PATCHED_BASE patch list (decoder_new.h:1142-1182), applied to the len8 values at n
+template <int NSLOT, int E, class OUT>
+__device__ __forceinline__ int body_patches(const InRing<NSLOT>& in, OUT& out, uint32_t n, uint32_t len8, uint32_t fbw,
+                                            uint32_t pw, uint32_t cfb, uint32_t pll, uint64_t base, uint32_t bit0,
+                                            uint32_t lane) {
+  constexpr uint64_t M = emask<E>();
+  // the reference masks patches with a 32-bit mask (decoder_new.h:1103)
+  const uint64_t pmask = pw >= 32 ? 0xffffffffull : ((1ull << pw) - 1ull);
+  uint64_t patch = 0;
+  uint32_t gap = 0;
+  if (lane < pll) {
+    const uint64_t ent = in.msb_bits64(bit0 + lane * cfb, cfb);
+    gap = static_cast<uint32_t>(shr64(ent, pw));
+    patch = shl64((ent & pmask) & M, fbw) & M;
+  }
+  uint32_t off = gap;  // inclusive scan of the gaps
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t o = __shfl_up_sync(FULL, off, d);
+    if (lane >= static_cast<uint32_t>(d)) off += o;
+  }
+  if (__any_sync(FULL, lane < pll && off >= len8)) return CODAG_ECORRUPT;
+  const uint32_t prev = __shfl_up_sync(FULL, off, 1);
+  if (__any_sync(FULL, lane > 0 && lane < pll && prev == off)) {
+    // several patches on one value: OR the group into its first lane
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint64_t o = shfl_down64(patch, d);
+      const uint32_t ooff = __shfl_down_sync(FULL, off, d);
+      if (lane + d < pll && ooff == off) patch |= o;
+    }
+  }
+  __syncwarp();
+  if (lane < pll && (lane == 0 || prev != off)) {
+    const uint64_t v = get_elem<E>(out, n + off);
+    put_elem<E>(out, n + off, ((((v - base) & M) | patch) + base) & M);
+  }
+  return CODAG_OK;
+}
+
+// RLE v1 literal group: `remaining` varints from pos (decoder.h:686-727); advances pos
+template <int NSLOT, int E, class OUT>
+__device__ __forceinline__ int body_literals(InRing<NSLOT>& in, OUT& out, uint32_t n, uint32_t remaining, uint32_t& pos,
+                                             uint32_t end, uint32_t lane) {
+  constexpr uint64_t M = emask<E>();
+  while (remaining) {
+    int st = in.advance(pos, min(pos + 148, end));
+    if (st) return st;
+    const uint32_t q0 = pos + 4 * lane;
+    const uint32_t tb = ~in.peek_le32(q0) & 0x80808080u;
+    uint32_t nib = ((tb >> 7) & 1u) | ((tb >> 14) & 2u) | ((tb >> 21) & 4u) | ((tb >> 28) & 8u);
+    if (q0 + 4 > end) nib &= q0 >= end ? 0u : ((1u << (end - q0)) - 1u);
+    const uint32_t b0 = __ballot_sync(FULL, nib & 1u), b1 = __ballot_sync(FULL, nib & 2u);
+    const uint32_t b2 = __ballot_sync(FULL, nib & 4u), b3 = __ballot_sync(FULL, nib & 8u);
+    const uint32_t lt = lanemask_lt(lane);
+    const uint32_t before = __popc(b0 & lt) + __popc(b1 & lt) + __popc(b2 & lt) + __popc(b3 & lt);
+    const uint32_t total = __popc(b0) + __popc(b1) + __popc(b2) + __popc(b3);
+    if (!total) return CODAG_ECORRUPT;  // a varint longer than 128 bytes
+    const uint32_t take = total < remaining ? total : remaining;
+    // end of the previous varint: the last end in a lower lane, or the window start
+    const uint32_t nz = __ballot_sync(FULL, nib != 0) & lt;
+    const uint32_t src = nz ? 31u - __clz(nz) : lane;
+    const uint32_t pnib = __shfl_sync(FULL, nib, src);
+    uint32_t start = nz ? pos + 4 * src + (32u - __clz(pnib)) : pos;
+    uint32_t m = nib, idx = before, last_end = 0;
+    while (m && idx < take) {
+      const uint32_t q = q0 + __ffs(m) - 1;
+      m &= m - 1;
+      const uint32_t len = q - start + 1;
+      uint64_t v;
+      if (len <= 4) {
+        v = leb_compact32(in.peek_le32(start), len);
+      } else {
+        const uint64_t lo8 = in.peek_le64(start);
+        v = leb_value(lo8, len > 8 ? in.peek_le64(start + 8) : 0ull, len);
+      }
+      put_elem<E>(out, n + idx, v & M);
+      if (idx == take - 1) last_end = q + 1;
+      idx++;
+      start = q + 1;
+    }
+    pos = __reduce_max_sync(FULL, last_end);
+    n += take;
+    remaining -= take;
+  }
+  return CODAG_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// single-pass decoders: the warp walks the headers itself
+// ---------------------------------------------------------------------------------------
+// RLE v1: loops while fewer than cap elements were produced, as the reference does
+// (decoder.h:669).
 template <int NSLOT, int E, class OUT>
 __device__ int decode_rlev1_chunk(InRing<NSLOT>& in, OUT& out, uint32_t cap) {
-  constexpr uint64_t M = emask<E>();
   const uint32_t lane = in.lane;
   const uint32_t end = in.hi;
   uint32_t pos = in.lo;
   uint32_t n = 0;
   int st = CODAG_OK;
-
   while (n < cap) {
     if (pos >= end) { st = CODAG_ECORRUPT; break; }
     st = in.advance(pos, min(pos + 32, end));
     if (st) break;
-    const uint32_t head = in.rd8(pos);
-    const int h = static_cast<int8_t>(head);
-    if (h >= 0) {
-      // run: count h+3, int8 delta, varint base (decoder.h:731-790)
+    const int h = static_cast<int8_t>(in.rd8(pos));
+    uint32_t cnt;
+    if (h >= 0) {  // run: count h+3, int8 delta, varint base (decoder.h:731-790)
       if (pos + 2 >= end) { st = CODAG_ECORRUPT; break; }
       const int64_t delta = static_cast<int8_t>(in.rd8(pos + 1));
       uint32_t len;
       uint64_t base;
       if (!read_uvarint(in, pos + 2, end, len, base)) { st = CODAG_ECORRUPT; break; }
-      const uint32_t cnt = static_cast<uint32_t>(h) + 3u;
+      cnt = static_cast<uint32_t>(h) + 3u;
       if (n + cnt > cap) { st = CODAG_ECORRUPT; break; }
-      uint64_t v = base + static_cast<uint64_t>(static_cast<int64_t>(lane) * delta);
-      const uint64_t step = static_cast<uint64_t>(32 * delta);
-      for (uint32_t i = lane; i < cnt; i += 32, v += step) put_elem<E>(out, n + i, v & M);
-      n += cnt;
+      body_fill<E>(out, n, cnt, base, static_cast<uint64_t>(delta), lane);
       pos += 2 + len;
     } else {
-      // literal group of -h varints (decoder.h:686-727), 128 stream bytes per step
-      uint32_t remaining = static_cast<uint32_t>(-h);
-      if (n + remaining > cap) { st = CODAG_ECORRUPT; break; }
+      cnt = static_cast<uint32_t>(-h);
+      if (n + cnt > cap) { st = CODAG_ECORRUPT; break; }
       pos += 1;
-      while (remaining) {
-        st = in.advance(pos, min(pos + 148, end));
-        if (st) break;
-        const uint32_t q0 = pos + 4 * lane;
-        const uint32_t w4 = static_cast<uint32_t>(in.peek_le64(q0));
-        const uint32_t tb = ~w4 & 0x80808080u;
-        uint32_t nib = ((tb >> 7) & 1u) | ((tb >> 14) & 2u) | ((tb >> 21) & 4u) | ((tb >> 28) & 8u);
-        if (q0 + 4 > end) nib &= q0 >= end ? 0u : ((1u << (end - q0)) - 1u);
-        const uint32_t b0 = __ballot_sync(FULL, nib & 1u), b1 = __ballot_sync(FULL, nib & 2u);
-        const uint32_t b2 = __ballot_sync(FULL, nib & 4u), b3 = __ballot_sync(FULL, nib & 8u);
-        const uint32_t lt = lanemask_lt(lane);
-        const uint32_t before = __popc(b0 & lt) + __popc(b1 & lt) + __popc(b2 & lt) + __popc(b3 & lt);
-        const uint32_t total = __popc(b0) + __popc(b1) + __popc(b2) + __popc(b3);
-        if (!total) { st = CODAG_ECORRUPT; break; }  // a varint longer than 128 bytes
-        const uint32_t take = total < remaining ? total : remaining;
-        // end of the previous varint: the last end in a lower lane, or the window start
-        const uint32_t nz = __ballot_sync(FULL, nib != 0) & lt;
-        const uint32_t src = nz ? 31u - __clz(nz) : lane;
-        const uint32_t pnib = __shfl_sync(FULL, nib, src);
-        uint32_t start = nz ? pos + 4 * src + (32u - __clz(pnib)) : pos;
-        uint32_t m = nib, idx = before, last_end = 0;
-        while (m) {
-          const uint32_t q = q0 + __ffs(m) - 1;
-          m &= m - 1;
-          if (idx < take) {
-            const uint32_t len = q - start + 1;
-            const uint64_t lo8 = in.peek_le64(start);
-            const uint64_t hi8 = len > 8 ? in.peek_le64(start + 8) : 0ull;
-            put_elem<E>(out, n + idx, leb_value(lo8, hi8, len) & M);
-            if (idx == take - 1) last_end = q + 1;
-          }
-          idx++;
-          start = q + 1;
-        }
-        pos = __reduce_max_sync(FULL, last_end);
-        n += take;
-        remaining -= take;
-      }
+      st = body_literals<NSLOT, E>(in, out, n, cnt, pos, end, lane);
       if (st) break;
     }
+    n += cnt;
     __syncwarp();
-    out.flush_to(static_cast<uint64_t>(n) * E);
+    out.flush_to(n * E);
   }
   if (!in.drain() && st == CODAG_OK) st = CODAG_ETIMEOUT;
-  out.finish(static_cast<uint64_t>(n) * E);
-  if (st == CODAG_OK && static_cast<uint64_t>(n) * E < out.store) st = CODAG_ECORRUPT;
+  out.finish(n * E);
+  if (st == CODAG_OK && n * E < out.store) st = CODAG_ECORRUPT;
   return st;
 }
 
-// ---------------------------------------------------------------------------------------
-// ORC RLE v2 (unsigned values, include/rlev2/decoder_new.h:909-1187)
-// ---------------------------------------------------------------------------------------
+// RLE v2 (unsigned values, include/rlev2/decoder_new.h:909-1187)
 template <int NSLOT, int E, class OUT>
 __device__ int decode_rlev2_chunk(InRing<NSLOT>& in, OUT& out, uint32_t cap) {
   constexpr uint64_t M = emask<E>();
@@ -205,7 +351,6 @@ __device__ int decode_rlev2_chunk(InRing<NSLOT>& in, OUT& out, uint32_t cap) {
   uint32_t pos = in.lo;
   uint32_t n = 0;
   int st = CODAG_OK;
-
   while (pos < end) {
     st = in.advance(pos, min(pos + 32, end));
     if (st) break;
@@ -214,7 +359,6 @@ __device__ int decode_rlev2_chunk(InRing<NSLOT>& in, OUT& out, uint32_t cap) {
     // the length field is held in a uint8_t (decoder_new.h:1019,1048,1095)
     const uint32_t len8 = ((static_cast<uint32_t>(hdr >> 48) & 0x1ffu) + 1u) & 0xffu;
     uint32_t cnt, total;
-
     if ((first >> 6) == 0) {  // SHORT_REPEAT (decoder_new.h:1004-1014)
       const uint32_t nb = ((first >> 3) & 7u) + 1u;
       cnt = (first & 7u) + 3u;
@@ -229,12 +373,7 @@ __device__ int decode_rlev2_chunk(InRing<NSLOT>& in, OUT& out, uint32_t cap) {
       if (pos + total > end || n + cnt > cap) { st = CODAG_ECORRUPT; break; }
       st = in.advance(pos, pos + total);
       if (st) break;
-      const uint32_t bit0 = (pos + 2u) * 8u;
-      if (fbw <= 32) {
-        for (uint32_t j = lane; j < cnt; j += 32) put_elem<E>(out, n + j, in.msb_bits32(bit0 + j * fbw, fbw) & M);
-      } else {
-        for (uint32_t j = lane; j < cnt; j += 32) put_elem<E>(out, n + j, in.msb_bits64(bit0 + j * fbw, fbw) & M);
-      }
+      body_unpack<NSLOT, E>(in, out, n, cnt, (pos + 2u) * 8u, fbw, 0ull, lane);
     } else if ((first >> 6) == 3) {  // DELTA (decoder_new.h:1044-1091)
       const uint32_t enc = (first >> 1) & 0x1fu;
       const uint32_t fbw = v2_width(enc);
@@ -254,26 +393,8 @@ __device__ int decode_rlev2_chunk(InRing<NSLOT>& in, OUT& out, uint32_t cap) {
       if (pos + total > end || n + cnt > cap) { st = CODAG_ECORRUPT; break; }
       st = in.advance(pos, pos + total);
       if (st) break;
-      if (enc == 0) {
-        uint64_t v = base + static_cast<uint64_t>(lane) * bd;
-        const uint64_t step = 32ull * bd;
-        for (uint32_t t = lane; t < cnt; t += 32, v += step) put_elem<E>(out, n + t, v & M);
-      } else {
-        const bool plus = bd != 0;  // multiplier = base_delta > 0 ? 1 : -1 on the unsigned type
-        const uint64_t v1 = (base + bd) & M;
-        if (lane == 0) put_elem<E>(out, n, base);
-        if (lane == 1) put_elem<E>(out, n + 1, v1);
-        uint64_t carry = v1;
-        const uint32_t bit0 = data * 8u;
-        for (uint32_t k0 = 0; k0 < nd; k0 += 32) {
-          const uint32_t k = k0 + lane;
-          const uint64_t d = k < nd ? (in.msb_bits64(bit0 + k * fbw, fbw) & M) : 0ull;
-          const uint64_t s = warp_scan_add64(d, lane);
-          const uint64_t v = (plus ? carry + s : carry - s) & M;
-          if (k < nd) put_elem<E>(out, n + 2 + k, v);
-          carry = shfl64(v, 31);
-        }
-      }
+      if (enc == 0) body_fill<E>(out, n, cnt, base, bd, lane);
+      else body_delta_packed<NSLOT, E>(in, out, n, nd, fbw, base, bd, data * 8u, lane);
     } else {  // PATCHED_BASE (decoder_new.h:1092-1183)
       const uint32_t fbw = v2_width((first >> 1) & 0x1fu);
       const uint32_t third = static_cast<uint32_t>(hdr >> 40) & 0xffu;
@@ -292,55 +413,21 @@ __device__ int decode_rlev2_chunk(InRing<NSLOT>& in, OUT& out, uint32_t cap) {
       st = in.advance(pos, pos + total);
       if (st) break;
       const uint64_t base = in.peek_be64(pos + 4) >> (64u - 8u * bw);
-      if (fbw <= 32) {
-        for (uint32_t j = lane; j < cnt; j += 32)
-          put_elem<E>(out, n + j, (in.msb_bits32(vals * 8u + j * fbw, fbw) + base) & M);
-      } else {
-        for (uint32_t j = lane; j < cnt; j += 32)
-          put_elem<E>(out, n + j, (in.msb_bits64(vals * 8u + j * fbw, fbw) + base) & M);
-      }
+      body_unpack<NSLOT, E>(in, out, n, cnt, vals * 8u, fbw, base, lane);
       if (pll) {
-        // the reference masks patches with a 32-bit mask (decoder_new.h:1103)
-        const uint64_t pmask = pw >= 32 ? 0xffffffffull : ((1ull << pw) - 1ull);
-        uint64_t patch = 0;
-        uint32_t gap = 0;
-        if (lane < pll) {
-          const uint64_t ent = in.msb_bits64(patches * 8u + lane * cfb, cfb);
-          gap = static_cast<uint32_t>(shr64(ent, pw));
-          patch = shl64((ent & pmask) & M, fbw) & M;
-        }
-        uint32_t off = gap;  // inclusive scan of the gaps (each below 2^8)
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-          const uint32_t o = __shfl_up_sync(FULL, off, d);
-          if (lane >= static_cast<uint32_t>(d)) off += o;
-        }
-        if (__any_sync(FULL, lane < pll && off >= len8)) { st = CODAG_ECORRUPT; break; }
-        const uint32_t prev = __shfl_up_sync(FULL, off, 1);
-        if (__any_sync(FULL, lane > 0 && lane < pll && prev == off)) {
-          // several patches on one value: OR the group into its first lane
-#pragma unroll
-          for (int d = 1; d < 32; d <<= 1) {
-            const uint64_t o = shfl_down64(patch, d);
-            const uint32_t ooff = __shfl_down_sync(FULL, off, d);
-            if (lane + d < pll && ooff == off) patch |= o;
-          }
-        }
         __syncwarp();
-        if (lane < pll && (lane == 0 || prev != off)) {
-          const uint64_t v = get_elem<E>(out, n + off);
-          put_elem<E>(out, n + off, ((((v - base) & M) | patch) + base) & M);
-        }
+        st = body_patches<NSLOT, E>(in, out, n, len8, fbw, pw, cfb, pll, base, patches * 8u, lane);
+        if (st) break;
       }
     }
     n += cnt;
     pos += total;
     __syncwarp();
-    out.flush_to(static_cast<uint64_t>(n) * E);
+    out.flush_to(n * E);
   }
   if (!in.drain() && st == CODAG_OK) st = CODAG_ETIMEOUT;
-  out.finish(static_cast<uint64_t>(n) * E);
-  if (st == CODAG_OK && static_cast<uint64_t>(n) * E < out.store) st = CODAG_ECORRUPT;
+  out.finish(n * E);
+  if (st == CODAG_OK && n * E < out.store) st = CODAG_ECORRUPT;
   return st;
 }
 

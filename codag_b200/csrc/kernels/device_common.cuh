@@ -65,6 +65,50 @@ __device__ __forceinline__ void bulk_g2s(void* smem_dst, const void* gsrc, uint3
       : "memory");
 }
 
+// Shared-memory accessors on 32-bit shared addresses (explicit ld/st.shared, no generic
+// addressing).  Loads are volatile asm, so they stay ordered after the (volatile) barrier
+// waits without pinning surrounding arithmetic; stores also clobber memory.
+__device__ __forceinline__ uint32_t ld_s8(uint32_t a) {
+  uint32_t v;
+  asm volatile("ld.shared.u8 %0, [%1];" : "=r"(v) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ uint32_t ld_s16(uint32_t a) {
+  uint32_t v;
+  asm volatile("ld.shared.u16 %0, [%1];" : "=r"(v) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ uint32_t ld_s32(uint32_t a) {
+  uint32_t v;
+  asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ uint64_t ld_s64(uint32_t a) {
+  uint64_t v;
+  asm volatile("ld.shared.u64 %0, [%1];" : "=l"(v) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ uint4 ld_s128(uint32_t a) {
+  uint4 v;
+  asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ void st_s8(uint32_t a, uint32_t v) {
+  asm volatile("st.shared.u8 [%0], %1;" ::"r"(a), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_s16(uint32_t a, uint32_t v) {
+  asm volatile("st.shared.u16 [%0], %1;" ::"r"(a), "h"(static_cast<unsigned short>(v)) : "memory");
+}
+__device__ __forceinline__ void st_s32(uint32_t a, uint32_t v) {
+  asm volatile("st.shared.u32 [%0], %1;" ::"r"(a), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_s64(uint32_t a, uint64_t v) {
+  asm volatile("st.shared.u64 [%0], %1;" ::"r"(a), "l"(v) : "memory");
+}
+__device__ __forceinline__ void st_g128(void* p, uint4 v) {
+  asm volatile("st.global.v4.u32 [%0], {%1, %2, %3, %4};" ::"l"(p), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w) : "memory");
+}
+
 __device__ __forceinline__ uint64_t bswap64(uint64_t v) {
   const uint32_t lo = static_cast<uint32_t>(v), hi = static_cast<uint32_t>(v >> 32);
   return (static_cast<uint64_t>(__byte_perm(lo, 0, 0x0123)) << 32) | __byte_perm(hi, 0, 0x0123);
@@ -123,6 +167,7 @@ struct InRing {
   static_assert((NSLOT & (NSLOT - 1)) == 0, "ring depth must be a power of two");
 
   uint8_t* buf;            // kBytes of shared memory, 16-byte aligned
+  uint32_t sbuf;           // shared-space address of buf
   uint64_t* bar;           // NSLOT mbarriers
   const uint8_t* gbase;    // stream start rounded down to 16 bytes
   uint32_t lo, hi;         // stream bytes are [lo, hi) relative to gbase
@@ -165,12 +210,12 @@ struct InRing {
     if (s == 0 && lane < 16) {
       const uint32_t p = lo + lane;
       const uint32_t head_end = body_lo < hi ? body_lo : hi;
-      if (p < head_end) buf[p & kMask] = gbase[p];
+      if (p < head_end) st_s8(sbuf + (p & kMask), gbase[p]);
     }
     const uint32_t tail_lo = body_hi > body_lo ? body_hi : body_lo;
     if (tail_lo < hi && s == ((hi - 1) >> kSlotLog2) && lane < 16) {
       const uint32_t p = tail_lo + lane;
-      if (p < hi) buf[p & kMask] = gbase[p];
+      if (p < hi) st_s8(sbuf + (p & kMask), gbase[p]);
     }
     if (lane == 0) {
       fence_proxy_async_smem();
@@ -241,10 +286,8 @@ struct InRing {
     return ok;
   }
 
-  __device__ __forceinline__ uint32_t rd8(uint32_t p) const { return buf[p & kMask]; }
-  __device__ __forceinline__ uint32_t rd32(uint32_t p4) const {
-    return *reinterpret_cast<const uint32_t*>(buf + (p4 & kMask));
-  }
+  __device__ __forceinline__ uint32_t rd8(uint32_t p) const { return ld_s8(sbuf + (p & kMask)); }
+  __device__ __forceinline__ uint32_t rd32(uint32_t p4) const { return ld_s32(sbuf + (p4 & kMask)); }
   // bytes p..p+7, little-endian
   __device__ __forceinline__ uint64_t peek_le64(uint32_t p) const {
     const uint32_t a = p & ~3u;
@@ -254,6 +297,11 @@ struct InRing {
     return sh ? (v >> sh) | (static_cast<uint64_t>(w2) << (64 - sh)) : v;
   }
   __device__ __forceinline__ uint64_t peek_be64(uint32_t p) const { return bswap64(peek_le64(p)); }
+  // bytes p..p+3, little-endian (two aligned loads)
+  __device__ __forceinline__ uint32_t peek_le32(uint32_t p) const {
+    const uint32_t a = p & ~3u;
+    return __funnelshift_r(rd32(a), rd32(a + 4), (p & 3u) * 8u);
+  }
   // big-endian 32-bit word at a 4-byte aligned position
   __device__ __forceinline__ uint32_t be32(uint32_t p4) const { return __byte_perm(rd32(p4), 0, 0x0123); }
   // w (1..32) bits at stream bit bitpos, most significant bit first (two aligned loads)
@@ -298,46 +346,44 @@ struct OutRing {
   static constexpr uint32_t kFlush = 1u << LOG2_FLUSH;
 
   uint8_t* buf;     // kBytes of shared memory, 16-byte aligned
+  uint32_t sbuf;    // shared-space address of buf
   uint8_t* gdst;    // chunk output base
-  uint64_t store;   // bytes of this chunk that may be stored
-  uint64_t flushed; // bytes already copied out (multiple of kFlush until the end)
+  uint32_t store;   // bytes of this chunk that may be stored (chunks are < 2 GiB)
+  uint32_t flushed; // bytes already copied out (multiple of kFlush until the end)
   uint32_t lane;
 
   __device__ __forceinline__ void begin(uint8_t* dst, uint64_t store_bytes) {
     gdst = dst;
-    store = store_bytes;
+    store = static_cast<uint32_t>(store_bytes);
     flushed = 0;
   }
 
   // copy [a, a+len) of the stream out of the ring; the range never wraps the ring
-  __device__ __forceinline__ void copy_out(uint64_t a, uint32_t len) {
+  __device__ __forceinline__ void copy_out(uint32_t a, uint32_t len) {
     if (a >= store) return;
-    if (a + len > store) len = static_cast<uint32_t>(store - a);
-    const uint8_t* src = buf + (a & kMask);
+    if (len > store - a) len = store - a;
+    const uint32_t src = sbuf + static_cast<uint32_t>(a & kMask);
     uint8_t* dst = gdst + a;
     const uintptr_t al = reinterpret_cast<uintptr_t>(dst);
     uint32_t done = 0;
     if ((al & 15u) == 0) {
       const uint32_t n16 = len >> 4;
-      for (uint32_t k = lane; k < n16; k += 32)
-        reinterpret_cast<uint4*>(dst)[k] = reinterpret_cast<const uint4*>(src)[k];
+      for (uint32_t k = lane; k < n16; k += 32) st_g128(dst + 16 * k, ld_s128(src + 16 * k));
       done = n16 << 4;
     } else if ((al & 7u) == 0) {
       const uint32_t n8 = len >> 3;
-      for (uint32_t k = lane; k < n8; k += 32)
-        reinterpret_cast<uint2*>(dst)[k] = reinterpret_cast<const uint2*>(src)[k];
+      for (uint32_t k = lane; k < n8; k += 32) reinterpret_cast<uint64_t*>(dst)[k] = ld_s64(src + 8 * k);
       done = n8 << 3;
     } else if ((al & 3u) == 0) {
       const uint32_t n4 = len >> 2;
-      for (uint32_t k = lane; k < n4; k += 32)
-        reinterpret_cast<uint32_t*>(dst)[k] = reinterpret_cast<const uint32_t*>(src)[k];
+      for (uint32_t k = lane; k < n4; k += 32) reinterpret_cast<uint32_t*>(dst)[k] = ld_s32(src + 4 * k);
       done = n4 << 2;
     }
-    for (uint32_t k = done + lane; k < len; k += 32) dst[k] = src[k];
+    for (uint32_t k = done + lane; k < len; k += 32) dst[k] = static_cast<uint8_t>(ld_s8(src + k));
   }
 
   // drains every complete flush piece below `pos`
-  __device__ __forceinline__ void flush_to(uint64_t pos) {
+  __device__ __forceinline__ void flush_to(uint32_t pos) {
     if (pos - flushed < kFlush) return;
     __syncwarp();
     do {
@@ -347,31 +393,16 @@ struct OutRing {
     __syncwarp();
   }
 
-  __device__ __forceinline__ void finish(uint64_t pos) {
+  __device__ __forceinline__ void finish(uint32_t pos) {
     __syncwarp();
-    if (pos > flushed) copy_out(flushed, static_cast<uint32_t>(pos - flushed));
+    if (pos > flushed) copy_out(flushed, pos - flushed);
     flushed = pos;
     __syncwarp();
   }
 
-  __device__ __forceinline__ void put(uint64_t idx, uint64_t v, int e) {
-    const uint32_t o = static_cast<uint32_t>(idx * static_cast<uint32_t>(e)) & kMask;
-    switch (e) {
-      case 8: *reinterpret_cast<uint64_t*>(buf + o) = v; break;
-      case 4: *reinterpret_cast<uint32_t*>(buf + o) = static_cast<uint32_t>(v); break;
-      case 2: *reinterpret_cast<uint16_t*>(buf + o) = static_cast<uint16_t>(v); break;
-      default: buf[o] = static_cast<uint8_t>(v); break;
-    }
-  }
-  __device__ __forceinline__ uint64_t get(uint64_t idx, int e) const {
-    const uint32_t o = static_cast<uint32_t>(idx * static_cast<uint32_t>(e)) & kMask;
-    switch (e) {
-      case 8: return *reinterpret_cast<const uint64_t*>(buf + o);
-      case 4: return *reinterpret_cast<const uint32_t*>(buf + o);
-      case 2: return *reinterpret_cast<const uint16_t*>(buf + o);
-      default: return buf[o];
-    }
-  }
+  // byte at stream position p of the window
+  __device__ __forceinline__ uint32_t get8(uint64_t p) const { return ld_s8(sbuf + static_cast<uint32_t>(p & kMask)); }
+  __device__ __forceinline__ void put8(uint64_t p, uint32_t v) { st_s8(sbuf + static_cast<uint32_t>(p & kMask), v); }
 };
 
 }  // namespace codag_dev

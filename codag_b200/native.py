@@ -18,7 +18,7 @@ RLEV1, RLEV2, DEFLATE = 0, 1, 2
 
 # every symbol declared in include/codag.h
 EXPORTS = (
-    "codag_decompress_rlev1", "codag_decompress_rlev2", "codag_decompress_deflate",
+    "codag_decompress_rlev1", "codag_decompress_rlev2", "codag_decompress_deflate", "codag_workspace_bytes",
     "codag_set_tune", "codag_get_tune", "codag_set_wait_limit", "codag_selftest_wait_timeout",
     "codag_batch_plan", "codag_batch_run", "codag_batch_destroy",
     "codag_hbuf_free", "codag_encode_rlev1", "codag_encode_rlev2", "codag_encode_deflate", "codag_encode_one",
@@ -61,7 +61,9 @@ def lib() -> C.CDLL:
         raise RuntimeError(f"{LIB_PATH} is missing: run `python -m codag_b200.build` (the decoders have no fallback)")
     L = C.CDLL(str(LIB_PATH))
     u64, i32, vp = C.c_uint64, C.c_int32, C.c_void_p
-    rle = [vp, u64, vp, vp, u64, u64, C.c_int, vp, u64, vp, vp]
+    rle = [vp, u64, vp, vp, u64, u64, C.c_int, vp, u64, vp, vp, u64, vp]
+    L.codag_workspace_bytes.argtypes = [C.c_int, u64]
+    L.codag_workspace_bytes.restype = u64
     for name in ("codag_decompress_rlev1", "codag_decompress_rlev2"):
         getattr(L, name).argtypes = rle
         getattr(L, name).restype = i32

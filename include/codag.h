@@ -2,8 +2,8 @@
  * codag.h -- C ABI of the B200-native CODAG chunk decompressors.
  *
  * Every pointer named d_* is a DEVICE pointer owned by the caller.  Calls are asynchronous
- * on `stream` (a cudaStream_t; NULL = legacy default stream), allocate no device memory,
- * never print and never exit.  The return value reports argument and launch errors only;
+ * on `stream` (a cudaStream_t; NULL = legacy default stream), allocate no device memory
+ * (scratch comes from the caller's workspace), never print and never exit.  The return value reports argument and launch errors only;
  * stream corruption and bounded-wait timeouts are reported per chunk in d_chunk_status
  * (CODAG_OK / CODAG_ECORRUPT / CODAG_ETIMEOUT), which may be NULL when not wanted.
  * Distinct streams may be used from distinct host threads concurrently.
@@ -46,11 +46,15 @@ enum { CODAG_CODEC_RLEV1 = 0, CODAG_CODEC_RLEV2 = 1, CODAG_CODEC_DEFLATE = 2 };
  *   d_col_len   n_chunks exact stream lengths in bytes
  *   chunk_bytes decoded bytes per chunk (131072 in CODAG), a multiple of elem_bytes
  *   elem_bytes  1, 2, 4 or 8 (the DATA_TYPE template argument)
+ *   d_workspace optional scratch of codag_workspace_bytes(codec, n_chunks) bytes, 256-byte
+ *               aligned; with it the headers are walked one thread per chunk before the
+ *               warp-per-chunk expansion (faster); NULL decodes in a single pass
  */
 codag_status codag_decompress_rlev1(const uint8_t *d_comp, uint64_t comp_bytes,
                                     const uint64_t *d_blk_off, const uint64_t *d_col_len,
                                     uint64_t n_chunks, uint64_t chunk_bytes, int elem_bytes,
                                     uint8_t *d_out, uint64_t out_bytes, int32_t *d_chunk_status,
+                                    void *d_workspace, uint64_t workspace_bytes,
                                     codag_stream_t stream);
 
 /*
@@ -59,12 +63,17 @@ codag_status codag_decompress_rlev1(const uint8_t *d_comp, uint64_t comp_bytes,
  * arguments (in, n_chunks, blk_off, col_len, CHUNK_SIZE) map one to one onto these.
  *   d_blk_off   n_chunks offsets (128-byte aligned in CODAG's layout)
  *   d_col_len   n_chunks exact stream lengths
+ *   d_workspace as for codag_decompress_rlev1
  */
 codag_status codag_decompress_rlev2(const uint8_t *d_comp, uint64_t comp_bytes,
                                     const uint64_t *d_blk_off, const uint64_t *d_col_len,
                                     uint64_t n_chunks, uint64_t chunk_bytes, int elem_bytes,
                                     uint8_t *d_out, uint64_t out_bytes, int32_t *d_chunk_status,
+                                    void *d_workspace, uint64_t workspace_bytes,
                                     codag_stream_t stream);
+
+/* Workspace bytes the two-pass RLE decode of n_chunks chunks uses (0 for Deflate). */
+uint64_t codag_workspace_bytes(int codec, uint64_t n_chunks);
 
 /*
  * Deflate, one stream per chunk.

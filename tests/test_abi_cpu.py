@@ -24,9 +24,9 @@ def test_exports_every_declared_symbol(native):
 def test_argument_validation_without_gpu(native):
     lib = native.lib()
     # null pointers / bad element widths are rejected before any CUDA call
-    assert lib.codag_decompress_rlev1(None, 0, None, None, 1, 131072, 8, None, 0, None, None) == native.EINVAL
-    assert lib.codag_decompress_rlev2(1, 1, 1, 1, 1, 131072, 3, 1, 1, None, None) == native.EINVAL
-    assert lib.codag_decompress_rlev2(1, 1, 1, 1, 1, 131071, 8, 1, 1, None, None) == native.EINVAL
+    assert lib.codag_decompress_rlev1(None, 0, None, None, 1, 131072, 8, None, 0, None, None, 0, None) == native.EINVAL
+    assert lib.codag_decompress_rlev2(1, 1, 1, 1, 1, 131072, 3, 1, 1, None, None, 0, None) == native.EINVAL
+    assert lib.codag_decompress_rlev2(1, 1, 1, 1, 1, 131071, 8, 1, 1, None, None, 0, None) == native.EINVAL
     assert lib.codag_decompress_deflate(1, 1, 1, 1, 131072, -1, 1, 1, None, None) == native.EINVAL
     bad = native.Tune(0, 4, 10, 0)
     assert lib.codag_set_tune(0, C.byref(bad)) == native.EINVAL
@@ -34,7 +34,9 @@ def test_argument_validation_without_gpu(native):
     assert lib.codag_set_tune(0, C.byref(bad)) == native.EINVAL
     assert lib.codag_set_wait_limit(0) == native.EINVAL
     # zero chunks is a no-op
-    assert lib.codag_decompress_rlev1(1, 1, 1, 1, 0, 131072, 8, 1, 1, None, None) == native.OK
+    assert lib.codag_decompress_rlev1(1, 1, 1, 1, 0, 131072, 8, 1, 1, None, None, 0, None) == native.OK
+    assert lib.codag_workspace_bytes(native.RLEV2, 8192) >= 8192 * 512 * 32
+    assert lib.codag_workspace_bytes(native.DEFLATE, 8192) == 0
 
 
 def test_tune_round_trip(native):

@@ -22,8 +22,9 @@ def _t(cuda, a, dtype=None):
     return cuda.from_numpy(a).to("cuda")
 
 
-def _gpu_rle(cuda, api, codec, comp, off, ln, chunk, e, out_bytes=None, comp_shift=0):
-    """Decode n RLE chunks on the GPU; comp_shift moves the whole stream buffer off 16-byte alignment."""
+def _gpu_rle(cuda, api, codec, comp, off, ln, chunk, e, out_bytes=None, comp_shift=0, two_pass=True):
+    """Decode n RLE chunks on the GPU; comp_shift moves the whole stream buffer off 16-byte alignment;
+    two_pass=False decodes without a workspace (the warp walks the headers itself)."""
     n = ln.size
     buf = np.zeros(comp.size + comp_shift, np.uint8)
     buf[comp_shift:] = comp
@@ -33,7 +34,8 @@ def _gpu_rle(cuda, api, codec, comp, off, ln, chunk, e, out_bytes=None, comp_shi
     out = cuda.full((total + 64,), 0xA5, dtype=cuda.uint8, device="cuda")
     st = cuda.full((n,), -1, dtype=cuda.int32, device="cuda")
     fn = api.decompress_rlev1 if codec == RLEV1 else api.decompress_rlev2
-    fn(d_comp, _t(cuda, off[:n]), _t(cuda, ln), chunk, e, out, total, st)
+    kw = {"ws": api.AUTO_WORKSPACE} if two_pass else {}
+    fn(d_comp, _t(cuda, off[:n]), _t(cuda, ln), chunk, e, out, total, st, **kw)
     cuda.cuda.synchronize()
     o = out.cpu().numpy()
     assert np.all(o[total:] == 0xA5), "wrote past out_bytes"
@@ -47,20 +49,23 @@ def api(native, cuda):
 
 
 # --- known-answer vectors --------------------------------------------------------------------
+@pytest.mark.parametrize("two_pass", [True, False])
 @pytest.mark.parametrize("name", sorted(VECTORS))
-def test_known_answer_vectors(cuda, api, name):
+def test_known_answer_vectors(cuda, api, name, two_pass):
     codec, e, stream, expected = VECTORS[name]
     want = _bytes_of(expected, e)
     s = np.array(stream, np.uint8)
-    st, out = _gpu_rle(cuda, api, codec, s, np.array([0], np.uint64), np.array([s.size], np.uint64), want.size, e)
+    st, out = _gpu_rle(cuda, api, codec, s, np.array([0], np.uint64), np.array([s.size], np.uint64), want.size, e,
+                       two_pass=two_pass)
     assert st.tolist() == [0]
     assert np.array_equal(out, want)
 
 
 # --- RLE v1 / v2 ----------------------------------------------------------------------------------
+@pytest.mark.parametrize("two_pass", [True, False])
 @pytest.mark.parametrize("e", [1, 2, 4, 8])
 @pytest.mark.parametrize("codec", [RLEV1, RLEV2])
-def test_rle_parity(native, oracle, cuda, api, codec, e):
+def test_rle_parity(native, oracle, cuda, api, codec, e, two_pass):
     n = (4 << 20) // e
     if codec == RLEV1:
         col = native.gen_rlev1_column(n, 31 + e, e)
@@ -70,7 +75,7 @@ def test_rle_parity(native, oracle, cuda, api, codec, e):
         col = native.gen_rlev2_column(n, 37 + e, e)
         comp, off, ln = native.encode_rlev2(col, CH, e)
     nch = ln.size
-    st, out = _gpu_rle(cuda, api, codec, comp, off, ln, CH, e)
+    st, out = _gpu_rle(cuda, api, codec, comp, off, ln, CH, e, two_pass=two_pass)
     assert not st.any()
     assert np.array_equal(out[:col.size], col)
     ref = np.zeros(nch * CH, np.uint8)
@@ -108,7 +113,8 @@ def test_rle_odd_chunk_sizes(native, oracle, cuda, api):
         assert np.array_equal(out1[:col1.size], col1)
 
 
-def test_rle_malformed_streams(native, cuda, api):
+@pytest.mark.parametrize("two_pass", [True, False])
+def test_rle_malformed_streams(native, cuda, api, two_pass):
     """Malformed chunks report ECORRUPT; their neighbours still decode; nothing faults."""
     col = native.gen_rlev2_column(16384 * 4, 5, 8)
     comp, off, ln = native.encode_rlev2(col, CH, 8)
@@ -118,7 +124,7 @@ def test_rle_malformed_streams(native, cuda, api):
     comp[int(off[2])] = 0x5E             # DIRECT header: 128 16-bit values, more than the stream has
     comp[int(off[2]) + 1] = 0x7F
     ln[2] = 4
-    st, out = _gpu_rle(cuda, api, RLEV2, comp, off, ln, CH, 8)
+    st, out = _gpu_rle(cuda, api, RLEV2, comp, off, ln, CH, 8, two_pass=two_pass)
     assert st[1] == 2 and st[2] == 2
     ok = [i for i in range(ln.size) if i not in (1, 2)]
     assert not st[ok].any()
@@ -131,8 +137,8 @@ def test_rle_malformed_streams(native, cuda, api):
     garbage = rng.integers(0, 256, size=64 * 1024, dtype=np.uint8)
     offs = np.arange(0, 64 * 1024, 4096, dtype=np.uint64)
     lens = np.full(offs.size, 4096, np.uint64)
-    st1, _ = _gpu_rle(cuda, api, RLEV1, garbage, offs, lens, 2048, 8)
-    st2, _ = _gpu_rle(cuda, api, RLEV2, garbage, offs, lens, 2048, 8)
+    st1, _ = _gpu_rle(cuda, api, RLEV1, garbage, offs, lens, 2048, 8, two_pass=two_pass)
+    st2, _ = _gpu_rle(cuda, api, RLEV2, garbage, offs, lens, 2048, 8, two_pass=two_pass)
     assert set(st1.tolist()) <= {0, 2} and set(st2.tolist()) <= {0, 2}
 
 
