@@ -48,7 +48,8 @@ enum { CODAG_CODEC_RLEV1 = 0, CODAG_CODEC_RLEV2 = 1, CODAG_CODEC_DEFLATE = 2 };
  *   elem_bytes  1, 2, 4 or 8 (the DATA_TYPE template argument)
  *   d_workspace optional scratch of codag_workspace_bytes(codec, n_chunks) bytes, 256-byte
  *               aligned; with it the headers are walked one thread per chunk before the
- *               warp-per-chunk expansion (faster); NULL decodes in a single pass
+ *               warp-per-chunk expansion; NULL decodes each chunk in a single warp pass,
+ *               which measures faster on B200 (the walk is bound by dependent global loads)
  */
 codag_status codag_decompress_rlev1(const uint8_t *d_comp, uint64_t comp_bytes,
                                     const uint64_t *d_blk_off, const uint64_t *d_col_len,
