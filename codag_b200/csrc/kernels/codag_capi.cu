@@ -270,8 +270,8 @@ codag_status finish_launch() {
 }
 
 // workspace of the two-pass RLE path: per-chunk descriptor counts, then descriptor tables
-uint64_t rle_ws_counts_bytes(uint64_t n) { return (n * 4 + 255) / 256 * 256; }
-uint64_t rle_ws_bytes(uint64_t n) { return rle_ws_counts_bytes(n) + n * kDescPerChunk * sizeof(RleDesc); }
+constexpr uint64_t rle_ws_counts_bytes(uint64_t n) { return (n * 4 + 255) / 256 * 256; }
+constexpr uint64_t rle_ws_bytes(uint64_t n) { return rle_ws_counts_bytes(n) + n * kDescPerChunk * sizeof(RleDesc); }
 
 template <int NSLOT, int CODEC, int E>
 codag_status launch_rle(const codag_tune& t, const uint8_t* comp, uint64_t comp_bytes, const uint64_t* blk_off,
@@ -365,6 +365,55 @@ extern "C" codag_status codag_decompress_rlev2(const uint8_t* d_comp, uint64_t c
                                                codag_stream_t stream) {
   return dispatch_rle<CODAG_CODEC_RLEV2>(d_comp, comp_bytes, d_blk_off, d_col_len, n_chunks, chunk_bytes, elem_bytes,
                                          d_out, out_bytes, d_chunk_status, d_workspace, workspace_bytes,
+                                         reinterpret_cast<cudaStream_t>(stream));
+}
+
+// ---------------------------------------------------------------------------------------
+// Two-pass RLE v2 decode for callers that cannot allocate device memory.
+//
+// The scratch is a fixed array in the module's device memory, sized for
+// CODAG_NOALLOC_MAX_CHUNKS chunks; every device that loads this library holds it until the
+// process exits.  In host code `g_noalloc_ws` only names a host-side shadow, so the device
+// address is looked up once per device with cudaGetSymbolAddress (on the first call made
+// with that device current) and passed to the kernels.  All calls share the array: the
+// header walk rewrites the count of every chunk it is given before the expansion reads it,
+// so no clearing is needed, and calls that overlap on the GPU race on the array.
+// ---------------------------------------------------------------------------------------
+namespace {
+constexpr uint64_t kNoAllocScratchBytes = rle_ws_bytes(CODAG_NOALLOC_MAX_CHUNKS);
+__device__ __align__(256) uint8_t g_noalloc_ws[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+codag_status noalloc_scratch(void** addr) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return CODAG_ECUDA;
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return CODAG_EINVAL;
+  std::lock_guard<std::mutex> g(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_ws) != cudaSuccess || !p) return CODAG_ECUDA;
+    g_noalloc_addr[dev] = p;
+  }
+  *addr = g_noalloc_addr[dev];
+  return CODAG_OK;
+}
+}  // namespace
+
+extern "C" codag_status codag_decompress_rlev2_noalloc(const uint8_t* d_comp, uint64_t comp_bytes,
+                                                       const uint64_t* d_blk_off, const uint64_t* d_col_len,
+                                                       uint64_t n_chunks, uint64_t chunk_bytes, int elem_bytes,
+                                                       uint8_t* d_out, uint64_t out_bytes, int32_t* d_chunk_status,
+                                                       codag_stream_t stream) {
+  if (n_chunks > CODAG_NOALLOC_MAX_CHUNKS) return CODAG_ELIMIT;
+  if (n_chunks == 0) return CODAG_OK;
+  void* ws = nullptr;
+  const codag_status st = noalloc_scratch(&ws);
+  if (st != CODAG_OK) return st;
+  return dispatch_rle<CODAG_CODEC_RLEV2>(d_comp, comp_bytes, d_blk_off, d_col_len, n_chunks, chunk_bytes, elem_bytes,
+                                         d_out, out_bytes, d_chunk_status, ws, kNoAllocScratchBytes,
                                          reinterpret_cast<cudaStream_t>(stream));
 }
 

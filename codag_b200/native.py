@@ -12,13 +12,16 @@ import numpy as np
 
 LIB_PATH = Path(__file__).resolve().parent / "libcodag_b200.so"
 
-OK, EINVAL, ECORRUPT, ETIMEOUT, ECUDA, ENOMEM = 0, 1, 2, 3, 4, 5
-STATUS_NAMES = {OK: "OK", EINVAL: "EINVAL", ECORRUPT: "ECORRUPT", ETIMEOUT: "ETIMEOUT", ECUDA: "ECUDA", ENOMEM: "ENOMEM"}
+OK, EINVAL, ECORRUPT, ETIMEOUT, ECUDA, ENOMEM, ELIMIT = 0, 1, 2, 3, 4, 5, 6
+STATUS_NAMES = {OK: "OK", EINVAL: "EINVAL", ECORRUPT: "ECORRUPT", ETIMEOUT: "ETIMEOUT", ECUDA: "ECUDA", ENOMEM: "ENOMEM",
+                ELIMIT: "ELIMIT"}
+NOALLOC_MAX_CHUNKS = 512  # CODAG_NOALLOC_MAX_CHUNKS
 RLEV1, RLEV2, DEFLATE = 0, 1, 2
 
 # every symbol declared in include/codag.h
 EXPORTS = (
     "codag_decompress_rlev1", "codag_decompress_rlev2", "codag_decompress_deflate", "codag_workspace_bytes",
+    "codag_decompress_rlev2_noalloc",
     "codag_set_tune", "codag_get_tune", "codag_set_wait_limit", "codag_selftest_wait_timeout",
     "codag_batch_plan", "codag_batch_run", "codag_batch_destroy",
     "codag_hbuf_free", "codag_encode_rlev1", "codag_encode_rlev2", "codag_encode_deflate", "codag_encode_one",
@@ -67,6 +70,8 @@ def lib() -> C.CDLL:
     for name in ("codag_decompress_rlev1", "codag_decompress_rlev2"):
         getattr(L, name).argtypes = rle
         getattr(L, name).restype = i32
+    L.codag_decompress_rlev2_noalloc.argtypes = [vp, u64, vp, vp, u64, u64, C.c_int, vp, u64, vp, vp]
+    L.codag_decompress_rlev2_noalloc.restype = i32
     L.codag_decompress_deflate.argtypes = [vp, u64, vp, u64, u64, C.c_int, vp, u64, vp, vp]
     L.codag_decompress_deflate.restype = i32
     L.codag_set_tune.argtypes = [C.c_int, C.POINTER(Tune)]

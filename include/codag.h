@@ -31,7 +31,8 @@ typedef enum {
     CODAG_ECORRUPT = 2, /* malformed stream (per chunk) */
     CODAG_ETIMEOUT = 3, /* a bounded device wait ran out (per chunk) */
     CODAG_ECUDA = 4,    /* a CUDA runtime call or launch failed */
-    CODAG_ENOMEM = 5    /* host allocation failed (planning calls only) */
+    CODAG_ENOMEM = 5,   /* host allocation failed (planning calls only) */
+    CODAG_ELIMIT = 6    /* request exceeds a fixed capacity (codag_decompress_rlev2_noalloc) */
 } codag_status;
 
 enum { CODAG_CODEC_RLEV1 = 0, CODAG_CODEC_RLEV2 = 1, CODAG_CODEC_DEFLATE = 2 };
@@ -75,6 +76,29 @@ codag_status codag_decompress_rlev2(const uint8_t *d_comp, uint64_t comp_bytes,
 
 /* Workspace bytes the two-pass RLE decode of n_chunks chunks uses (0 for Deflate). */
 uint64_t codag_workspace_bytes(int codec, uint64_t n_chunks);
+
+/*
+ * RLE v2 two-pass decode that allocates nothing.  No counterpart in CODAG: it exists for
+ * callers that cannot call cudaMalloc -- a plugin inside a host engine whose device memory
+ * is all reserved by that engine's own pool, or code that must not allocate at all on its
+ * path -- and so cannot hand codag_decompress_rlev2 a workspace.
+ * Arguments and output are those of codag_decompress_rlev2 without the workspace.  The
+ * scratch is a fixed array of codag_workspace_bytes(CODAG_CODEC_RLEV2,
+ * CODAG_NOALLOC_MAX_CHUNKS) bytes (about 8 MiB) in the library's device memory, which every
+ * device that loads the library holds until the process exits.
+ *   - n_chunks above CODAG_NOALLOC_MAX_CHUNKS returns CODAG_ELIMIT (split the request).
+ *   - The first call on a device looks up the array's device address on that device
+ *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *   - Every call shares the one array and leaves its contents behind.  Calls whose work
+ *     overlaps on the GPU (different streams, or different host threads) race on it:
+ *     order them on one stream or with events.
+ */
+#define CODAG_NOALLOC_MAX_CHUNKS 512
+codag_status codag_decompress_rlev2_noalloc(const uint8_t *d_comp, uint64_t comp_bytes,
+                                            const uint64_t *d_blk_off, const uint64_t *d_col_len,
+                                            uint64_t n_chunks, uint64_t chunk_bytes, int elem_bytes,
+                                            uint8_t *d_out, uint64_t out_bytes,
+                                            int32_t *d_chunk_status, codag_stream_t stream);
 
 /*
  * Deflate, one stream per chunk.
