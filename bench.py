@@ -340,17 +340,21 @@ def main():
     ap.add_argument("--tune", default="", help="explicit launch shape warps_per_cta,ring_slots,lut_bits")
     ap.add_argument("--n-values", type=int, default=None,
                     help="override the workload's element count (profiling cases; not a bench line)")
+    ap.add_argument("--n-files", type=int, default=None, help="batched: number of files (default 20,000)")
+    ap.add_argument("--per-file-sample", type=int, default=600,
+                    help="batched: files timed through the per-file path (stratified sample)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.workload == "batched":
-        from codag_b200 import batched_bench
-        return batched_bench.main(args, rank, world, local)
     if args.impl == "reference":
         if rank == 0:
-            run_reference(args)
+            if args.workload == "batched":
+                from codag_b200 import batched_bench
+                batched_bench.run_reference(args)
+            else:
+                run_reference(args)
         return
     if world > 1:
         import torch
@@ -358,7 +362,11 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     try:
-        run_ours(args, rank, world, local)
+        if args.workload == "batched":
+            from codag_b200 import batched_bench
+            batched_bench.main(args, rank, world, local)
+        else:
+            run_ours(args, rank, world, local)
     finally:
         if world > 1:
             import torch.distributed as dist

@@ -160,3 +160,55 @@ extern "C" codag_status codag_encode_one(int codec, const uint8_t* in, uint64_t 
   if (rc != CODAG_OK) return static_cast<codag_status>(rc);
   return to_hbuf(out.data(), out.size(), stream) ? CODAG_OK : CODAG_ENOMEM;
 }
+
+extern "C" codag_status codag_encode_set(const uint8_t* in, const uint64_t* in_off, const uint64_t* in_len,
+                                         const uint8_t* codecs, const uint8_t* elem_bytes, uint64_t n, int level,
+                                         codag_chunk_desc* descs, codag_hbuf* comp, uint64_t* out_bytes) {
+  if (!in || !in_off || !in_len || !codecs || !elem_bytes || !descs || !comp || !out_bytes || n == 0 || level < 0 ||
+      level > 9)
+    return CODAG_EINVAL;
+  for (uint64_t i = 0; i < n; i++) {
+    if (in_len[i] == 0 || in_len[i] > 0xffffffffull || codecs[i] > CODAG_CODEC_DEFLATE) return CODAG_EINVAL;
+    if (codecs[i] != CODAG_CODEC_DEFLATE && (!valid_elem(elem_bytes[i]) || in_len[i] % elem_bytes[i]))
+      return CODAG_EINVAL;
+  }
+  std::vector<std::vector<uint8_t>> streams(n);
+  int failed = 0;
+#pragma omp parallel for schedule(dynamic, 4) reduction(| : failed)
+  for (int64_t i = 0; i < static_cast<int64_t>(n); i++) {
+    const uint8_t* src = in + in_off[i];
+    int rc;
+    if (codecs[i] == CODAG_CODEC_RLEV1) {
+      rc = rlev1_encode_chunk(src, in_len[i], elem_bytes[i], streams[i]);
+    } else if (codecs[i] == CODAG_CODEC_RLEV2) {
+      rc = rlev2_encode_chunk(src, in_len[i], elem_bytes[i], streams[i]);
+    } else {
+      uint32_t types = 0;
+      rc = deflate_encode_chunk(src, in_len[i], level, 1, Z_DEFAULT_STRATEGY, streams[i], &types);
+    }
+    failed |= rc != CODAG_OK || streams[i].size() > 0xffffffffull;
+  }
+  if (failed) return CODAG_EINVAL;
+  uint64_t c = 0, o = 0;
+  for (uint64_t i = 0; i < n; i++) {
+    codag_chunk_desc& d = descs[i];
+    std::memset(&d, 0, sizeof(d));
+    d.comp_off = c;
+    d.comp_len = static_cast<uint32_t>(streams[i].size());
+    d.out_off = o;
+    d.out_len = static_cast<uint32_t>(in_len[i]);
+    d.codec = codecs[i];
+    d.elem_bytes = codecs[i] == CODAG_CODEC_DEFLATE ? 1 : elem_bytes[i];
+    d.wrapper_bytes = codecs[i] == CODAG_CODEC_DEFLATE ? 2 : 0;
+    c += round_up(streams[i].size(), 16);
+    o += round_up(in_len[i], 256);
+  }
+  comp->data = static_cast<uint8_t*>(std::calloc(c ? c : 1, 1));
+  comp->bytes = c;
+  if (!comp->data) return CODAG_ENOMEM;
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < static_cast<int64_t>(n); i++)
+    if (!streams[i].empty()) std::memcpy(comp->data + descs[i].comp_off, streams[i].data(), streams[i].size());
+  *out_bytes = o;
+  return CODAG_OK;
+}

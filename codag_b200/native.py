@@ -25,6 +25,7 @@ EXPORTS = (
     "codag_set_tune", "codag_get_tune", "codag_set_wait_limit", "codag_selftest_wait_timeout",
     "codag_batch_plan", "codag_batch_run", "codag_batch_destroy",
     "codag_hbuf_free", "codag_encode_rlev1", "codag_encode_rlev2", "codag_encode_deflate", "codag_encode_one",
+    "codag_encode_set",
     "codag_gen_rlev1_column", "codag_gen_rlev2_column", "codag_gen_text",
 )
 
@@ -92,7 +93,9 @@ def lib() -> C.CDLL:
     L.codag_encode_deflate.argtypes = [vp, u64, u64, C.c_int, C.c_int, C.c_int, C.POINTER(HBuf), C.POINTER(HBuf),
                                        C.POINTER(HBuf)]
     L.codag_encode_one.argtypes = [C.c_int, vp, u64, C.c_int, C.c_int, C.POINTER(HBuf)]
-    for name in ("codag_encode_rlev1", "codag_encode_rlev2", "codag_encode_deflate", "codag_encode_one"):
+    L.codag_encode_set.argtypes = [vp, vp, vp, vp, vp, u64, C.c_int, vp, C.POINTER(HBuf), C.POINTER(u64)]
+    for name in ("codag_encode_rlev1", "codag_encode_rlev2", "codag_encode_deflate", "codag_encode_one",
+                 "codag_encode_set"):
         getattr(L, name).restype = i32
     for name in ("codag_gen_rlev1_column", "codag_gen_rlev2_column"):
         getattr(L, name).argtypes = [u64, u64, C.c_int, vp]
@@ -160,6 +163,27 @@ def encode_one(codec: int, data: np.ndarray, elem_bytes: int = 8, level: int = 6
     b = HBuf()
     check("codag_encode_one", lib().codag_encode_one(codec, _ptr(raw), raw.nbytes, elem_bytes, level, C.byref(b)))
     return _take(b)
+
+
+def encode_set(src: np.ndarray, in_off: np.ndarray, in_len: np.ndarray, codecs: np.ndarray, elem_bytes: np.ndarray,
+               level: int = 6):
+    """Encodes independent files (slices of src) one stream each and packs them for a batch plan:
+    returns (comp, descs, out_bytes)."""
+    src = np.ascontiguousarray(src).view(np.uint8).reshape(-1)
+    in_off = np.ascontiguousarray(in_off, dtype=np.uint64)
+    in_len = np.ascontiguousarray(in_len, dtype=np.uint64)
+    codecs = np.ascontiguousarray(codecs, dtype=np.uint8)
+    elem_bytes = np.ascontiguousarray(elem_bytes, dtype=np.uint8)
+    n = in_off.size
+    if not (in_len.size == codecs.size == elem_bytes.size == n) or np.any(in_off + in_len > src.size):
+        raise ValueError("encode_set: inconsistent file table")
+    descs = np.zeros(n, dtype=CHUNK_DESC_DTYPE)
+    b = HBuf()
+    ob = C.c_uint64()
+    check("codag_encode_set", lib().codag_encode_set(_ptr(src), _ptr(in_off), _ptr(in_len), _ptr(codecs),
+                                                    _ptr(elem_bytes), n, level, descs.ctypes.data, C.byref(b),
+                                                    C.byref(ob)))
+    return _take(b), descs, int(ob.value)
 
 
 def gen_rlev1_column(n: int, seed: int, elem_bytes: int = 8) -> np.ndarray:

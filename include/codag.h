@@ -201,6 +201,15 @@ codag_status codag_encode_deflate(const uint8_t *in, uint64_t in_bytes, uint64_t
 codag_status codag_encode_one(int codec, const uint8_t *in, uint64_t in_bytes, int elem_bytes,
                               int level, codag_hbuf *stream);
 
+/* A set of n independent files, file i = in[in_off[i] .. +in_len[i]), each encoded as ONE
+ * stream of codecs[i] (Deflate: zlib level `level` with the 2-byte zlib wrapper; RLE:
+ * elem_bytes[i]-wide values) and packed for codag_batch_plan: streams 16-byte aligned in
+ * `comp`, outputs 256-byte aligned in an output buffer of *out_bytes; descs[i] is filled.
+ * OpenMP over files. */
+codag_status codag_encode_set(const uint8_t *in, const uint64_t *in_off, const uint64_t *in_len,
+                              const uint8_t *codecs, const uint8_t *elem_bytes, uint64_t n, int level,
+                              codag_chunk_desc *descs, codag_hbuf *comp, uint64_t *out_bytes);
+
 /* Seeded synthetic columns (splitmix64/xoshiro256**). */
 void codag_gen_rlev1_column(uint64_t n, uint64_t seed, int elem_bytes, uint8_t *out);
 void codag_gen_rlev2_column(uint64_t n, uint64_t seed, int elem_bytes, uint8_t *out);

@@ -1,0 +1,93 @@
+"""Mixed sets of independently compressed files: the set producer against the oracle (CPU),
+and the batched persistent launch and the per-file path against the source data (GPU)."""
+import numpy as np
+import pytest
+
+from codag_b200 import batched
+
+
+@pytest.fixture(scope="module")
+def small_set(native):
+    return batched.make_mixed_set(400, seed=99, max_bytes=256 << 10, source_bytes=8 << 20)
+
+
+def test_set_layout_and_oracle_round_trip(small_set, oracle):
+    ms = small_set
+    d = ms.descs
+    assert np.all(d["comp_off"] % 16 == 0) and np.all(d["out_off"] % 256 == 0)
+    assert np.all(d["out_len"] == ms.in_len) and np.all(ms.in_len % 8 == 0)
+    assert set(np.unique(d["codec"]).tolist()) == {0, 1, 2}
+    assert np.all((d["wrapper_bytes"] == 2) == (d["codec"] == 2))
+    assert np.all(np.isin(d["elem_bytes"][d["codec"] != 2], [4, 8]))
+    out = np.zeros(ms.out_bytes, np.uint8)
+    st = oracle.decode_batch(ms.comp, d["comp_off"], d["comp_len"], out, d["out_off"], d["out_len"], d["out_len"],
+                             d["codec"], d["elem_bytes"], d["wrapper_bytes"])
+    assert not st.any()
+    assert np.array_equal(out, ms.expected())
+
+
+def test_stratified_sample_covers_codecs(small_set):
+    s = batched.stratified_sample(small_set, 30)
+    assert s.size == 30 and np.all(np.diff(s) > 0)
+    assert set(small_set.codecs[s].tolist()) == {0, 1, 2}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("use_graph", [False, True])
+@pytest.mark.parametrize("shape", [None, (1, 4, 9), (4, 8, 11), (8, 4, 10)])
+def test_batched_matches_source(cuda, small_set, shape, use_graph):
+    from codag_b200 import api
+    ms = small_set
+    d_comp = cuda.from_numpy(ms.comp).to("cuda")
+    d_out = cuda.full((ms.out_bytes,), 0x77, dtype=cuda.uint8, device="cuda")
+    st = cuda.full((ms.n,), -1, dtype=cuda.int32, device="cuda")
+    plan = api.BatchPlan(ms.descs, *shape) if shape else api.BatchPlan(ms.descs)
+    try:
+        for _ in range(2):  # second run replays the graph over the first run's output
+            plan.run(d_comp, d_out, st, use_graph=use_graph)
+        cuda.cuda.synchronize()
+    finally:
+        plan.close()
+    assert not st.cpu().numpy().any()
+    got = d_out.cpu().numpy()
+    want = ms.expected()
+    for d, ln in zip(ms.descs, ms.in_len):
+        o = int(d["out_off"])
+        assert np.array_equal(got[o:o + int(ln)], want[o:o + int(ln)])
+
+
+@pytest.mark.gpu
+def test_per_file_path_matches_source(cuda, small_set):
+    ms = small_set
+    d_comp = cuda.from_numpy(ms.comp).to("cuda")
+    d_out = cuda.zeros((ms.out_bytes,), dtype=cuda.uint8, device="cuda")
+    pf = batched.PerFileDecoder(ms, d_comp, d_out, "cuda")
+    files = batched.stratified_sample(ms, 60)
+    pf.run(files, cuda.cuda.current_stream())
+    cuda.cuda.synchronize()
+    assert not pf.d_st.cpu().numpy()[files].any()
+    got = d_out.cpu().numpy()
+    for i in files:
+        o, ln, s = int(ms.descs["out_off"][i]), int(ms.in_len[i]), int(ms.in_off[i])
+        assert np.array_equal(got[o:o + ln], ms.src[s:s + ln])
+
+
+@pytest.mark.gpu
+def test_batched_reports_corrupt_file_and_decodes_the_rest(cuda, small_set):
+    from codag_b200 import api
+    ms = small_set
+    comp = ms.comp.copy()
+    bad = int(np.nonzero(ms.codecs == 2)[0][0])
+    d = ms.descs[bad]
+    comp[int(d["comp_off"]) + 2:int(d["comp_off"]) + int(d["comp_len"])] = 0xFF  # invalid block type 3
+    d_comp = cuda.from_numpy(comp).to("cuda")
+    d_out = cuda.zeros((ms.out_bytes,), dtype=cuda.uint8, device="cuda")
+    st = cuda.full((ms.n,), -1, dtype=cuda.int32, device="cuda")
+    plan = api.BatchPlan(ms.descs)
+    try:
+        plan.run(d_comp, d_out, st, use_graph=False)
+        cuda.cuda.synchronize()
+    finally:
+        plan.close()
+    s = st.cpu().numpy()
+    assert s[bad] == 2 and np.count_nonzero(s) == 1
