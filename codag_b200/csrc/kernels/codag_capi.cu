@@ -27,7 +27,7 @@ namespace {
 constexpr uint32_t align_up(uint32_t v, uint32_t a) { return (v + a - 1) / a * a; }
 
 using RleOut = OutRing<12, 10>;      // 4 KiB ring, 1 KiB drains
-using InflateOut = OutRing<13, 11>;  // 8 KiB window, 2 KiB drains
+using InflateOut = OutRing<12, 10>;  // 4 KiB window, 1 KiB drains (the batch kernel decodes RLE into it too)
 
 template <int NSLOT>
 struct RleLayout {
@@ -242,7 +242,7 @@ __global__ void k_selftest_timeout(int32_t* status, uint64_t wait_cycles) {
 // host side
 // ---------------------------------------------------------------------------------------
 std::mutex g_mu;
-codag_tune g_tune[3] = {{8, 4, 10, 0}, {8, 4, 10, 0}, {4, 4, 10, 0}};
+codag_tune g_tune[3] = {{8, 4, 10, 0}, {8, 4, 10, 0}, {2, 2, 9, 0}};
 uint64_t g_wait_cycles = 2000000000ull;  // about one second at 2 GHz
 
 bool valid_slots(int s) { return s == 2 || s == 4 || s == 8; }
@@ -421,7 +421,8 @@ extern "C" codag_status codag_decompress_deflate(const uint8_t* d_comp, uint64_t
                                                  uint64_t n_chunks, uint64_t chunk_bytes, int wrapper_bytes,
                                                  uint8_t* d_out, uint64_t out_bytes, int32_t* d_chunk_status,
                                                  codag_stream_t stream) {
-  if (!d_comp || !d_blk_off || (!d_out && out_bytes) || chunk_bytes == 0 || wrapper_bytes < 0 || wrapper_bytes > 16)
+  if (!d_comp || !d_blk_off || (!d_out && out_bytes) || chunk_bytes == 0 || chunk_bytes >= (1ull << 31) ||
+      wrapper_bytes < 0 || wrapper_bytes > 16)
     return CODAG_EINVAL;
   if (n_chunks == 0) return CODAG_OK;
   const codag_tune t = tune_of(CODAG_CODEC_DEFLATE);

@@ -8,9 +8,12 @@
 //     lengths and 8 bits for distances, in parallel over the warp (canonical codes are
 //     tiled in MSB-first order, so each table slot finds its code by walking lengths);
 //   - keeps a 64-bit bit buffer refilled 32 bits at a time from the TMA input ring;
-//   - expands back-references warp-cooperatively out of an 8 KiB shared-memory window of
-//     the output (older sources are read back from the chunk's already-written output);
-//   - drains output in 2 KiB pieces with 16-byte vector stores;
+//   - decodes a length or distance code together with its extra bits (one table entry
+//     gives both widths) and two literals per step where the table slot holds both codes;
+//   - expands back-references warp-cooperatively out of a 4 KiB shared-memory window of
+//     the output; older sources are read back from the chunk's already-written output,
+//     and such a load (length <= 32) is left in flight while the next symbols decode;
+//   - drains output in 1 KiB pieces with 16-byte vector stores;
 //   - decodes stored blocks.
 // Every lane runs the same symbol loop on the same data (shared-memory reads broadcast), so
 // control flow stays uniform and only the stores are lane-specific.
@@ -33,25 +36,50 @@ __constant__ uint8_t kCodeLenOrder[19] = {16, 17, 18, 0, 8, 7, 9, 6, 10, 5, 11, 
 constexpr uint32_t kDistLB = 8;
 constexpr uint32_t kCodeLenLB = 7;
 
-// table entry: [0,4) code length, [4,8) extra bits, [8,10) kind, [16,32) value
-enum : uint32_t { kKindLit = 0, kKindLen = 1, kKindEnd = 2, kKindBad = 3 };
+// Table entry (32 bits):
+//   [0,5)   bits consumed in all: code length + extra bits, or both codes of a literal pair
+//   [5,9)   code length of the (first) symbol
+//   [9,11)  kind: literal(s), length, end of block, other (invalid, or not in the table)
+//   [11]    a second literal follows in [24,32) (literal/length tables only)
+//   [12]    the code is longer than the table: decode it with slow_entry
+//   [16,32) literal byte in [16,24) / length or distance base / code-length symbol
+enum : uint32_t {
+  kKindShift = 9,
+  kKindMask = 3u << kKindShift,
+  kKindLitBits = 0u,
+  kKindLenBits = 1u << kKindShift,
+  kKindEndBits = 2u << kKindShift,
+  kKindBadBits = 3u << kKindShift,
+  kPairFlag = 1u << 11,
+  kSlowFlag = 1u << 12,
+  kSlowEntry = kKindBadBits | kSlowFlag,
+};
 enum : int { kAlphaLitLen = 0, kAlphaDist = 1, kAlphaCodeLen = 2 };
+
+__device__ __forceinline__ uint32_t entry_bits(uint32_t total, uint32_t len) { return total | (len << 5); }
 
 __device__ __forceinline__ uint32_t make_entry(uint32_t sym, uint32_t len, int alpha) {
   if (alpha == kAlphaLitLen) {
-    if (sym < 256) return len | (kKindLit << 8) | (sym << 16);
-    if (sym == 256) return len | (kKindEnd << 8);
+    if (sym < 256) return entry_bits(len, len) | kKindLitBits | (sym << 16);
+    if (sym == 256) return entry_bits(len, len) | kKindEndBits;
     if (sym <= 285) {
       const uint32_t k = sym - 257;
-      return len | (static_cast<uint32_t>(kLenExtra[k]) << 4) | (kKindLen << 8) | (static_cast<uint32_t>(kLenBase[k]) << 16);
+      return entry_bits(len + kLenExtra[k], len) | kKindLenBits | (static_cast<uint32_t>(kLenBase[k]) << 16);
     }
-    return len | (kKindBad << 8);
+    return entry_bits(len, len) | kKindBadBits;
   }
   if (alpha == kAlphaDist) {
-    if (sym < 30) return len | (static_cast<uint32_t>(kDistExtra[sym]) << 4) | (static_cast<uint32_t>(kDistBase[sym]) << 16);
-    return len | (kKindBad << 8);
+    if (sym < 30) return entry_bits(len + kDistExtra[sym], len) | (static_cast<uint32_t>(kDistBase[sym]) << 16);
+    return entry_bits(len, len) | kKindBadBits;
   }
-  return len | (sym << 16);
+  return entry_bits(len, len) | (sym << 16);
+}
+
+// `n` bits of `x` starting at bit `pos` (pos + n <= 32; n may be 0)
+__device__ __forceinline__ uint32_t bfe32(uint32_t x, uint32_t pos, uint32_t n) {
+  uint32_t r;
+  asm("bfe.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(x), "r"(pos), "r"(n));
+  return r;
 }
 
 struct HuffTable {
@@ -104,7 +132,7 @@ __device__ bool build_table(const uint8_t* lens, uint32_t nsym, const HuffTable&
   const uint32_t n = 1u << t.lb;
   for (uint32_t x = lane; x < n; x += 32) {
     const uint32_t v = __brev(x) >> (32 - t.lb);  // MSB-first code prefix of table slot x
-    uint32_t entry = 0;
+    uint32_t entry = kSlowEntry;
     for (uint32_t l = 1; l <= t.lb; l++) {
       const uint32_t k = (v >> (t.lb - l)) - t.first[l];
       if (k < t.cnt[l]) {
@@ -115,6 +143,21 @@ __device__ bool build_table(const uint8_t* lens, uint32_t nsym, const HuffTable&
     t.lut[x] = entry;
   }
   __syncwarp();
+  if (alpha == kAlphaLitLen) {
+    // literal pairs: when the bits of slot x after its literal code hold a whole literal
+    // code too, the entry carries both.  Only the first-literal fields of the other slot
+    // are read, and a pair rewrite leaves those fields unchanged, so lanes need no order.
+    for (uint32_t x = lane; x < n; x += 32) {
+      const uint32_t e1 = t.lut[x];
+      const uint32_t l1 = (e1 >> 5) & 15u;
+      if ((e1 & kKindMask) != kKindLitBits || l1 >= t.lb) continue;
+      const uint32_t e2 = t.lut[x >> l1];
+      const uint32_t l2 = (e2 >> 5) & 15u;
+      if ((e2 & kKindMask) != kKindLitBits || l1 + l2 > t.lb) continue;
+      t.lut[x] = (e1 & ~31u & 0x00ffffffu) | (l1 + l2) | kPairFlag | ((e2 & 0x00ff0000u) << 8);
+    }
+    __syncwarp();
+  }
   return true;
 }
 
@@ -184,7 +227,7 @@ template <int NSLOT, int LB, class OUT>
 __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<LB>& sc, uint64_t chunk_bytes,
                                     uint32_t wrapper) {
   const uint32_t lane = in.lane;
-  const uint64_t cap = chunk_bytes;
+  const uint32_t cap = static_cast<uint32_t>(chunk_bytes);
   const HuffTable lit{sc.lit_lut, sc.lit_sorted, sc.lit_cnt, sc.lit_first, sc.lit_index, LB};
   const HuffTable dst{sc.dist_lut, sc.dist_sorted, sc.dist_cnt, sc.dist_first, sc.dist_index, kDistLB};
   const HuffTable cl{sc.dist_lut, sc.dist_sorted, sc.dist_cnt, sc.dist_first, sc.dist_index, kCodeLenLB};
@@ -206,6 +249,19 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<
   if (br.bc < 32) {                      \
     st = br.refill(in);                  \
     if (st) break;                       \
+  }
+  // one deferred far copy: pend_len bytes for [pend_op, pend_end), byte `lane` in pend_val
+  uint32_t pend_op = 0, pend_len = 0, pend_end = 0, pend_val = 0;
+#define CODAG_COMPLETE()                                              \
+  if (pend_len) {                                                     \
+    if (lane < pend_len) out.put8(pend_op + lane, pend_val);          \
+    pend_len = 0;                                                     \
+    pend_end = 0;                                                     \
+  }
+#define CODAG_FLUSH()   \
+  {                     \
+    CODAG_COMPLETE();   \
+    out.flush_to(op);   \
   }
 
   bool last = false;
@@ -235,7 +291,7 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<
         p += piece;
         left -= piece;
         __syncwarp();
-        out.flush_to(op);
+        CODAG_FLUSH();
       }
       if (st) break;
       br.start(in, p);
@@ -282,8 +338,8 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<
       while (idx < total) {
         CODAG_REFILL();
         const uint32_t e = ld_s32(s_dist + 4u * static_cast<uint32_t>(br.bb & ((1u << kCodeLenLB) - 1u)));
-        if (!e) { st = CODAG_ECORRUPT; break; }
-        br.drop(e & 15u);
+        if (e & kSlowFlag) { st = CODAG_ECORRUPT; break; }  // code lengths are at most 7 bits
+        br.drop(e & 31u);
         const uint32_t sym = e >> 16;
         if (sym < 16) {
           if (lane == 0) sc.lens[idx] = static_cast<uint8_t>(sym);
@@ -327,69 +383,97 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<
     // symbol loop (zlib.h:712-805)
     for (;;) {
       CODAG_REFILL();
-      uint32_t e = ld_s32(s_lit + 4u * static_cast<uint32_t>(br.bb & ((1u << LB) - 1u)));
-      if (!e) {
-        e = slow_entry(br.bb, lit, kAlphaLitLen);
-        if (!e) { st = CODAG_ECORRUPT; break; }
-      }
-      const uint32_t kind = (e >> 8) & 3u;
-      br.drop(e & 15u);
-      if (kind == kKindLit) {
-        if (op >= cap) { st = CODAG_ECORRUPT; break; }
-        if (lane == 0) out.put8(op, e >> 16);
-        op++;
-        if (op - out.flushed >= OUT::kFlush) out.flush_to(op);
+      uint32_t e = ld_s32(s_lit + ((static_cast<uint32_t>(br.bb) & ((1u << LB) - 1u)) << 2));
+      if ((e & kKindMask) == kKindLitBits) {  // one literal or a pair
+        const uint32_t pair = (e >> 11) & 1u;
+        br.drop(e & 31u);
+        if (lane <= pair) out.put8(op + lane, lane ? e >> 24 : (e >> 16) & 0xffu);
+        op += 1u + pair;
+        if (op - out.flushed >= OUT::kFlush) CODAG_FLUSH();
         continue;
       }
-      if (kind == kKindEnd) break;
-      if (kind == kKindBad) { st = CODAG_ECORRUPT; break; }
-      const uint32_t lext = (e >> 4) & 15u;
-      const uint32_t len = (e >> 16) + (static_cast<uint32_t>(br.bb) & ((1u << lext) - 1u));
-      br.drop(lext);
-      CODAG_REFILL();
-      uint32_t d = ld_s32(s_dist + 4u * static_cast<uint32_t>(br.bb & ((1u << kDistLB) - 1u)));
-      if (!d) {
+      if (e & kSlowFlag) {
+        e = slow_entry(br.bb, lit, kAlphaLitLen);
+        if (!e) { st = CODAG_ECORRUPT; break; }
+        if ((e & kKindMask) == kKindLitBits) {
+          br.drop(e & 31u);
+          if (lane == 0) out.put8(op, (e >> 16) & 0xffu);
+          op++;
+          if (op - out.flushed >= OUT::kFlush) CODAG_FLUSH();
+          continue;
+        }
+      }
+      if ((e & kKindMask) == kKindEndBits) {
+        br.drop(e & 31u);
+        break;
+      }
+      if ((e & kKindMask) != kKindLenBits) { st = CODAG_ECORRUPT; break; }
+      // length: code and extra bits in one step (at most 20 bits; 32 are buffered)
+      const uint32_t ln = (e >> 5) & 15u, lt = e & 31u;
+      const uint32_t len = (e >> 16) + bfe32(static_cast<uint32_t>(br.bb), ln, lt - ln);
+      br.drop(lt);
+      if (br.bc < 28) {  // distance code and extra bits take at most 28 bits
+        st = br.refill(in);
+        if (st) break;
+      }
+      uint32_t d = ld_s32(s_dist + ((static_cast<uint32_t>(br.bb) & ((1u << kDistLB) - 1u)) << 2));
+      if (d & kSlowFlag) {
         d = slow_entry(br.bb, dst, kAlphaDist);
         if (!d) { st = CODAG_ECORRUPT; break; }
       }
-      if ((d >> 8) & 3u) { st = CODAG_ECORRUPT; break; }
-      br.drop(d & 15u);
-      const uint32_t dext = (d >> 4) & 15u;
-      const uint32_t dist = (d >> 16) + (static_cast<uint32_t>(br.bb) & ((1u << dext) - 1u));
-      br.drop(dext);
+      if (d & kKindMask) { st = CODAG_ECORRUPT; break; }
+      const uint32_t dn = (d >> 5) & 15u, dt = d & 31u;
+      const uint32_t dist = (d >> 16) + bfe32(static_cast<uint32_t>(br.bb), dn, dt - dn);
+      br.drop(dt);
       if (dist > op || op + len > cap) { st = CODAG_ECORRUPT; break; }
-      __syncwarp();
+      const uint32_t src = op - dist;
       if (dist + len <= OUT::kBytes) {  // source still in the shared-memory window
+        if (src < pend_end) CODAG_COMPLETE();
+        __syncwarp();
         if (dist >= len) {
-          for (uint32_t t = lane; t < len; t += 32) out.put8(op + t, out.get8(op - dist + t));
+          for (uint32_t t = lane; t < len; t += 32) out.put8(op + t, out.get8(src + t));
         } else {
           uint32_t r = lane % dist;
           const uint32_t step = 32u % dist;
           for (uint32_t t = lane; t < len; t += 32) {
-            out.put8(op + t, out.get8(op - dist + r));
+            out.put8(op + t, out.get8(src + r));
             r += step;
             if (r >= dist) r -= dist;
           }
         }
-      } else {  // older than the window: read back the chunk's flushed output
-        const uint64_t src0 = op - dist;
-        uint32_t r = dist >= len ? lane : lane % dist;
+      } else if (len <= 32) {
+        // older than the window: the bytes were flushed to the chunk's output already.  The
+        // load is issued now and its bytes enter the window later (CODAG_COMPLETE), so the
+        // memory latency overlaps the next symbols.
+        CODAG_COMPLETE();
+        pend_val = (lane < len && src + lane < out.store) ? static_cast<uint32_t>(out.gdst[src + lane]) : 0u;
+        pend_op = op;
+        pend_len = len;
+        pend_end = op + len;
+      } else {
+        CODAG_COMPLETE();
+        const uint32_t r0 = dist >= len ? lane : lane % dist;
         const uint32_t step = dist >= len ? 32u : 32u % dist;
+        uint32_t r = r0;
         for (uint32_t t = lane; t < len; t += 32) {
-          const uint64_t s = src0 + r;
-          out.put8(op + t, s < out.store ? out.gdst[s] : 0u);  // unstored bytes are never stored either
+          const uint32_t sp = src + r;
+          out.put8(op + t, sp < out.store ? out.gdst[sp] : 0u);  // unstored bytes are never stored either
           r += step;
           if (dist < len && r >= dist) r -= dist;
         }
       }
       op += len;
-      if (op - out.flushed >= OUT::kFlush) out.flush_to(op);
+      if (op - out.flushed >= OUT::kFlush) CODAG_FLUSH();
     }
   }
+  CODAG_COMPLETE();
+#undef CODAG_FLUSH
+#undef CODAG_COMPLETE
 #undef CODAG_REFILL
   if (!in.drain() && st == CODAG_OK) st = CODAG_ETIMEOUT;
   out.finish(op);
-  if (st == CODAG_OK && (op < out.store || br.bitpos() > static_cast<uint64_t>(in.hi) * 8u)) st = CODAG_ECORRUPT;
+  if (st == CODAG_OK && (op < out.store || op > cap || br.bitpos() > static_cast<uint64_t>(in.hi) * 8u))
+    st = CODAG_ECORRUPT;
   return st;
 }
 

@@ -401,8 +401,8 @@ struct OutRing {
   }
 
   // byte at stream position p of the window
-  __device__ __forceinline__ uint32_t get8(uint64_t p) const { return ld_s8(sbuf + static_cast<uint32_t>(p & kMask)); }
-  __device__ __forceinline__ void put8(uint64_t p, uint32_t v) { st_s8(sbuf + static_cast<uint32_t>(p & kMask), v); }
+  __device__ __forceinline__ uint32_t get8(uint32_t p) const { return ld_s8(sbuf + (p & kMask)); }
+  __device__ __forceinline__ void put8(uint32_t p, uint32_t v) { st_s8(sbuf + (p & kMask), v); }
 };
 
 }  // namespace codag_dev

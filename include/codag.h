@@ -45,7 +45,7 @@ enum { CODAG_CODEC_RLEV1 = 0, CODAG_CODEC_RLEV2 = 1, CODAG_CODEC_DEFLATE = 2 };
  *   comp_bytes  readable bytes at d_comp (every stream must lie inside)
  *   d_blk_off   n_chunks offsets: stream i starts at d_comp + d_blk_off[i]
  *   d_col_len   n_chunks exact stream lengths in bytes
- *   chunk_bytes decoded bytes per chunk (131072 in CODAG), a multiple of elem_bytes
+ *   chunk_bytes decoded bytes per chunk (131072 in CODAG), a multiple of elem_bytes, < 2^31
  *   elem_bytes  1, 2, 4 or 8 (the DATA_TYPE template argument)
  *   d_workspace optional scratch of codag_workspace_bytes(codec, n_chunks) bytes, 256-byte
  *               aligned; with it the headers are walked one thread per chunk before the
