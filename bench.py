@@ -332,7 +332,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="rlev2", choices=sorted(WORKLOADS) + ["batched"])
+    ap.add_argument("--workload", default="rlev2", choices=sorted(WORKLOADS) + ["batched", "serving"])
     ap.add_argument("--autotune", default="cached", choices=["cached", "search", ""],
                     help="pick the launch shape with the autotuner (cached result or a fresh search)")
     ap.add_argument("--rle-passes", type=int, default=1, choices=[1, 2],
@@ -343,6 +343,11 @@ def main():
     ap.add_argument("--n-files", type=int, default=None, help="batched: number of files (default 20,000)")
     ap.add_argument("--per-file-sample", type=int, default=600,
                     help="batched: files timed through the per-file path (stratified sample)")
+    ap.add_argument("--rates", default="50,100,200,500,1000,2000", help="serving: request rates (per second)")
+    ap.add_argument("--duration", type=float, default=60.0, help="serving: seconds of arrivals per rate")
+    ap.add_argument("--pool-files", type=int, default=48, help="serving: distinct request files")
+    ap.add_argument("--budget-gb", type=int, default=64, help="serving: output memory budget")
+    ap.add_argument("--slots", type=int, default=4, help="serving: launches in flight")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -365,6 +370,9 @@ def main():
         if args.workload == "batched":
             from codag_b200 import batched_bench
             batched_bench.main(args, rank, world, local)
+        elif args.workload == "serving":
+            from codag_b200 import serving_bench
+            serving_bench.main(args, rank, world, local)
         else:
             run_ours(args, rank, world, local)
     finally:

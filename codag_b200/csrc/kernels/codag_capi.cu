@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(256) k_batch(const codag_chunk_desc* __restric
     if (lane == 0) k = atomicAdd(queue, 1u);
     k = __shfl_sync(FULL, k, 0);
     if (k >= n) break;
-    const uint32_t i = order[k];
+    const uint32_t i = order ? order[k] : k;
     const codag_chunk_desc d = descs[i];
     int st;
     const bool out_ok = d.out_off <= out_bytes && d.out_len <= out_bytes - d.out_off;
@@ -650,4 +650,67 @@ extern "C" codag_status codag_batch_destroy(codag_plan* p) {
   if (p->d_queue) cudaFree(p->d_queue);
   delete p;
   return CODAG_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// launches over caller-owned descriptor lists (continuous batching)
+// ---------------------------------------------------------------------------------------
+namespace {
+struct LaunchShape {
+  codag_tune tune;
+  int grid_cap;  // SMs x resident CTAs of k_batch for this shape on the current device
+  int dev;
+};
+std::mutex g_shape_mu;
+std::vector<LaunchShape> g_shapes;
+
+codag_status launch_shape(const codag_tune& t, int* grid_cap) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return CODAG_ECUDA;
+  {
+    std::lock_guard<std::mutex> g(g_shape_mu);
+    for (const LaunchShape& s : g_shapes)
+      if (s.dev == dev && s.tune.warps_per_cta == t.warps_per_cta && s.tune.ring_slots == t.ring_slots &&
+          s.tune.lut_bits == t.lut_bits) {
+        *grid_cap = s.grid_cap;
+        return CODAG_OK;
+      }
+  }
+  codag_plan probe;
+  probe.n = 0xffffffffull;
+  probe.tune = t;
+  const codag_status st = batch_setup_any(&probe);
+  if (st != CODAG_OK) return st;
+  std::lock_guard<std::mutex> g(g_shape_mu);
+  g_shapes.push_back({t, probe.grid, dev});
+  *grid_cap = probe.grid;
+  return CODAG_OK;
+}
+}  // namespace
+
+extern "C" codag_status codag_batch_launch(const codag_chunk_desc* d_descs, const uint32_t* d_order, uint64_t n,
+                                           uint32_t* d_queue, const codag_tune* tune, const uint8_t* d_comp,
+                                           uint64_t comp_bytes, uint8_t* d_out, uint64_t out_bytes,
+                                           int32_t* d_status, codag_stream_t stream) {
+  if (!d_descs || !d_queue || !d_comp || !d_out || n > 0xffffffffull) return CODAG_EINVAL;
+  if (n == 0) return CODAG_OK;
+  codag_plan p;
+  p.n = n;
+  p.tune = tune ? *tune : tune_of(CODAG_CODEC_DEFLATE);
+  if (!valid_warps(p.tune.warps_per_cta) || !valid_slots(p.tune.ring_slots) || !valid_lut(p.tune.lut_bits))
+    return CODAG_EINVAL;
+  if (p.tune.ring_slots < 4) p.tune.ring_slots = 4;  // mixed batches include RLE chunks
+  int cap = 0;
+  const codag_status st = launch_shape(p.tune, &cap);
+  if (st != CODAG_OK) return st;
+  const uint64_t need = (n + p.tune.warps_per_cta - 1) / p.tune.warps_per_cta;
+  p.grid = static_cast<int>(std::min<uint64_t>(need, static_cast<uint64_t>(cap)));
+  p.d_descs = const_cast<codag_chunk_desc*>(d_descs);
+  p.d_order = const_cast<uint32_t*>(d_order);
+  p.d_queue = d_queue;
+  batch_enqueue(&p, d_comp, comp_bytes, d_out, out_bytes, d_status, reinterpret_cast<cudaStream_t>(stream));
+  p.d_descs = nullptr;  // borrowed: the destructor-free plan owns nothing
+  p.d_order = nullptr;
+  p.d_queue = nullptr;
+  return finish_launch();
 }

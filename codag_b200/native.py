@@ -23,7 +23,7 @@ EXPORTS = (
     "codag_decompress_rlev1", "codag_decompress_rlev2", "codag_decompress_deflate", "codag_workspace_bytes",
     "codag_decompress_rlev2_noalloc",
     "codag_set_tune", "codag_get_tune", "codag_set_wait_limit", "codag_selftest_wait_timeout",
-    "codag_batch_plan", "codag_batch_run", "codag_batch_destroy",
+    "codag_batch_plan", "codag_batch_run", "codag_batch_destroy", "codag_batch_launch",
     "codag_hbuf_free", "codag_encode_rlev1", "codag_encode_rlev2", "codag_encode_deflate", "codag_encode_one",
     "codag_encode_set",
     "codag_gen_rlev1_column", "codag_gen_rlev2_column", "codag_gen_text",
@@ -82,8 +82,9 @@ def lib() -> C.CDLL:
     L.codag_batch_plan.argtypes = [vp, u64, C.POINTER(Tune), C.POINTER(vp)]
     L.codag_batch_run.argtypes = [vp, vp, u64, vp, u64, vp, C.c_int, vp]
     L.codag_batch_destroy.argtypes = [vp]
+    L.codag_batch_launch.argtypes = [vp, vp, u64, vp, C.POINTER(Tune), vp, u64, vp, u64, vp, vp]
     for name in ("codag_set_tune", "codag_get_tune", "codag_set_wait_limit", "codag_selftest_wait_timeout",
-                 "codag_batch_plan", "codag_batch_run", "codag_batch_destroy"):
+                 "codag_batch_plan", "codag_batch_run", "codag_batch_destroy", "codag_batch_launch"):
         getattr(L, name).restype = i32
     L.codag_hbuf_free.argtypes = [C.POINTER(HBuf)]
     L.codag_hbuf_free.restype = None

@@ -171,6 +171,17 @@ codag_status codag_batch_run(codag_plan *plan, const uint8_t *d_comp, uint64_t c
                              codag_stream_t stream);
 codag_status codag_batch_destroy(codag_plan *plan);
 
+/* One persistent launch over n descriptors that already sit in device memory, for callers
+ * that rebuild the chunk list for every launch (continuous batching).  d_order (n u32,
+ * may be NULL = descriptor order) is the order the warps take chunks in; d_queue is 4 bytes
+ * of device memory that this call resets on `stream`; d_status has n entries (may be NULL)
+ * and entry i reports descriptor i.  tune may be NULL (process-wide defaults).  Allocates
+ * nothing; the launch shape of each tune is measured once per device and cached. */
+codag_status codag_batch_launch(const codag_chunk_desc *d_descs, const uint32_t *d_order, uint64_t n,
+                                uint32_t *d_queue, const codag_tune *tune, const uint8_t *d_comp,
+                                uint64_t comp_bytes, uint8_t *d_out, uint64_t out_bytes,
+                                int32_t *d_status, codag_stream_t stream);
+
 /* --- host-side format producers (CPU; used by the CLIs, tests and benchmarks) ---------- */
 typedef struct {
     uint8_t *data;
