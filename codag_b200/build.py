@@ -28,6 +28,7 @@ CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fopenmp", "-Wall", "-Wno-unused-fun
 
 HOST_SOURCES = sorted((CSRC / "host").glob("*.cpp"))
 CUDA_SOURCES = [CSRC / "kernels" / "codag_capi.cu"]
+CUDA = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 HEADERS = sorted(CSRC.rglob("*.cuh")) + sorted(CSRC.rglob("*.hpp")) + [REPO / "include" / "codag.h"]
 CLI_SOURCES = {name: CSRC / "cli" / f"{name}_main.cpp" for name in ("rlev1", "rlev2", "zlib")}
 
@@ -72,9 +73,10 @@ def build(force: bool = False, verbose: bool = False) -> Path:
             continue
         exe = EXE / name / f"{name}.cu.exe"
         exe.parent.mkdir(parents=True, exist_ok=True)
-        if force or _stale(exe, [src, LIB] + HEADERS):
-            _run(["g++", "-O2", "-std=c++17", src, "-I", REPO / "include", "-o", exe, "-L", PKG, "-lcodag_b200",
-                  f"-Wl,-rpath,{PKG}", "-Wl,-rpath,$ORIGIN/../../../../codag_b200"], verbose)
+        if force or _stale(exe, [src, LIB, CSRC / "cli" / "cli_common.hpp"] + HEADERS):
+            _run(["g++", "-O2", "-std=c++17", "-Wall", src, "-I", REPO / "include", "-I", CUDA / "include", "-o", exe,
+                  "-L", PKG, "-lcodag_b200", "-L", CUDA / "lib64", "-lcudart",
+                  "-Wl,-rpath,$ORIGIN/../../../../codag_b200", f"-Wl,-rpath,{CUDA / 'lib64'}"], verbose)
     return LIB
 
 
