@@ -37,10 +37,6 @@
  *     element type (decoder_new.h:1057).
  * Where the reference would read or write out of bounds on a malformed stream, the oracle
  * stops and returns ORC_ECORRUPT instead.
- *
- * Parity of this oracle is pinned by (a) round trips against the original columns, and
- * (b) golden outputs of the reference decoders themselves, rebuilt from the reference
- * sources by oracle/build_ref.sh and run on a B200 (tests/golden/).
  */
 #include <stdint.h>
 #include <stdlib.h>
