@@ -26,7 +26,7 @@ namespace {
 // ---------------------------------------------------------------------------------------
 constexpr uint32_t align_up(uint32_t v, uint32_t a) { return (v + a - 1) / a * a; }
 
-using RleOut = OutRing<12, 10>;      // 4 KiB ring, 1 KiB drains
+using RleOut = OutRing<12, 10, true>;  // 4 KiB ring, 1 KiB drains by TMA bulk stores
 using InflateOut = OutRing<12, 10>;  // 4 KiB window, 1 KiB drains (the batch kernel decodes RLE into it too)
 
 template <int NSLOT>

@@ -65,6 +65,19 @@ __device__ __forceinline__ void bulk_g2s(void* smem_dst, const void* gsrc, uint3
       : "memory");
 }
 
+// 1-D bulk copy shared -> global (TMA store), tracked in this thread's bulk async-group.
+// Both addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_s2g(void* gdst, uint32_t ssrc, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(ssrc), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// Waits until at most N of this thread's committed bulk groups still read shared memory.
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+
 // Shared-memory accessors on 32-bit shared addresses (explicit ld/st.shared, no generic
 // addressing).  Loads are volatile asm, so they stay ordered after the (volatile) barrier
 // waits without pinning surrounding arithmetic; stores also clobber memory.
@@ -339,11 +352,17 @@ __device__ __forceinline__ void init_ring_barriers(uint64_t* bar, uint32_t lane)
 // ---------------------------------------------------------------------------------------
 // output staging ring
 // ---------------------------------------------------------------------------------------
-template <int LOG2_BYTES, int LOG2_FLUSH>
+template <int LOG2_BYTES, int LOG2_FLUSH, bool BULK = false>
 struct OutRing {
   static constexpr uint32_t kBytes = 1u << LOG2_BYTES;
   static constexpr uint32_t kMask = kBytes - 1;
   static constexpr uint32_t kFlush = 1u << LOG2_FLUSH;
+  // BULK: complete pieces leave by TMA bulk stores issued by lane 0; no decoder may read
+  // the chunk's output back from global memory while the stores are in flight.  A piece
+  // may be rewritten once the store of the piece after it has been issued (the stores are
+  // waited for down to one in flight), which holds while a header writes at most
+  // kBytes - 2 * kFlush bytes past the last complete piece.
+  static_assert(LOG2_BYTES >= LOG2_FLUSH + 2, "ring must hold four flush pieces");
 
   uint8_t* buf;     // kBytes of shared memory, 16-byte aligned
   uint32_t sbuf;    // shared-space address of buf
@@ -366,18 +385,32 @@ struct OutRing {
     uint8_t* dst = gdst + a;
     const uintptr_t al = reinterpret_cast<uintptr_t>(dst);
     uint32_t done = 0;
-    if ((al & 15u) == 0) {
-      const uint32_t n16 = len >> 4;
-      for (uint32_t k = lane; k < n16; k += 32) st_g128(dst + 16 * k, ld_s128(src + 16 * k));
-      done = n16 << 4;
-    } else if ((al & 7u) == 0) {
-      const uint32_t n8 = len >> 3;
-      for (uint32_t k = lane; k < n8; k += 32) reinterpret_cast<uint64_t*>(dst)[k] = ld_s64(src + 8 * k);
-      done = n8 << 3;
-    } else if ((al & 3u) == 0) {
-      const uint32_t n4 = len >> 2;
-      for (uint32_t k = lane; k < n4; k += 32) reinterpret_cast<uint32_t*>(dst)[k] = ld_s32(src + 4 * k);
-      done = n4 << 2;
+    if constexpr (BULK) {
+      if ((al & 15u) == 0 && len >= 16) {
+        fence_proxy_async_smem();  // this lane's ring writes become visible to the bulk copy
+        __syncwarp();
+        done = len & ~15u;
+        if (lane == 0) {
+          bulk_s2g(dst, src, done);
+          bulk_commit();
+          bulk_wait_read<1>();
+        }
+      }
+    }
+    if (!done) {
+      if ((al & 15u) == 0) {
+        const uint32_t n16 = len >> 4;
+        for (uint32_t k = lane; k < n16; k += 32) st_g128(dst + 16 * k, ld_s128(src + 16 * k));
+        done = n16 << 4;
+      } else if ((al & 7u) == 0) {
+        const uint32_t n8 = len >> 3;
+        for (uint32_t k = lane; k < n8; k += 32) reinterpret_cast<uint64_t*>(dst)[k] = ld_s64(src + 8 * k);
+        done = n8 << 3;
+      } else if ((al & 3u) == 0) {
+        const uint32_t n4 = len >> 2;
+        for (uint32_t k = lane; k < n4; k += 32) reinterpret_cast<uint32_t*>(dst)[k] = ld_s32(src + 4 * k);
+        done = n4 << 2;
+      }
     }
     for (uint32_t k = done + lane; k < len; k += 32) dst[k] = static_cast<uint8_t>(ld_s8(src + k));
   }
@@ -397,6 +430,9 @@ struct OutRing {
     __syncwarp();
     if (pos > flushed) copy_out(flushed, pos - flushed);
     flushed = pos;
+    if constexpr (BULK) {
+      if (lane == 0) bulk_wait_read<0>();  // the ring is reused by the next chunk
+    }
     __syncwarp();
   }
 
