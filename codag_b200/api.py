@@ -161,6 +161,87 @@ def decompress_deflate_host(comp: np.ndarray, blk_offset: np.ndarray, chunk_byte
     return out.cpu().numpy()
 
 
+# --- host buffers in, host buffer out, with copies and decode overlapped -------------------------
+class HostPipeline:
+    """Decodes a chunked file from pinned host memory into pinned host memory.
+
+    The chunks are split into `groups`; group g's compressed bytes go up, its chunks are
+    decoded and its output comes down on stream g % streams, so the host-to-device copy of
+    one group, the decode of another and the device-to-host copy of a third overlap (the
+    two copy directions run on separate copy engines).  Device buffers are kept between
+    calls and grow as needed.  The streams of a chunk must be laid out in chunk order (as in
+    every CODAG layout), so each group's compressed bytes are one contiguous range.
+    """
+
+    def __init__(self, codec: int, chunk_bytes: int = 131072, elem_bytes: int = 8, wrapper_bytes: int = 2,
+                 groups: int = 8, streams: int = 3, device="cuda"):
+        self.codec, self.chunk, self.elem, self.wrapper = codec, chunk_bytes, elem_bytes, wrapper_bytes
+        self.groups, self.dev = groups, torch.device(device)
+        self.streams = [torch.cuda.Stream(device=self.dev) for _ in range(streams)]
+        self.d_comp = self.d_out = self.d_off = self.d_len = self.d_st = None
+
+    def _grow(self, name, n, dtype):
+        t = getattr(self, name)
+        if t is None or t.numel() < n:
+            t = torch.empty(max(n, 1), dtype=dtype, device=self.dev)
+            setattr(self, name, t)
+        return t
+
+    def run(self, h_comp: torch.Tensor, h_off: torch.Tensor, h_len: torch.Tensor | None, out_bytes: int,
+            h_out: torch.Tensor, off_np: np.ndarray, len_np: np.ndarray | None) -> None:
+        """h_comp/h_out pinned uint8; h_off/h_len pinned int64 (RLE: n offsets and lengths;
+        Deflate: n+1 offsets, h_len None); off_np/len_np the same metadata on the host, used to
+        find each group's byte range.  Returns after the output is in h_out; raises CodagError
+        with the per-chunk status attached if a chunk failed."""
+        deflate = self.codec == native.DEFLATE
+        n = h_off.numel() - 1 if deflate else h_len.numel()
+        ch = self.chunk
+        d_comp = self._grow("d_comp", h_comp.numel(), torch.uint8)
+        d_out = self._grow("d_out", n * ch, torch.uint8)
+        d_off = self._grow("d_off", h_off.numel(), torch.int64)
+        d_len = self._grow("d_len", 0 if deflate else h_len.numel(), torch.int64)
+        d_st = self._grow("d_st", n, torch.int32)
+        main = torch.cuda.current_stream(self.dev)
+        s0 = self.streams[0]
+        s0.wait_stream(main)
+        with torch.cuda.stream(s0):
+            d_off[:h_off.numel()].copy_(h_off, non_blocking=True)
+            if not deflate:
+                d_len[:h_len.numel()].copy_(h_len, non_blocking=True)
+        meta = torch.cuda.Event()
+        meta.record(s0)
+        lib = native.lib()
+        bounds = np.linspace(0, n, min(self.groups, n) + 1).astype(np.int64)
+        for g in range(bounds.size - 1):
+            a, b = int(bounds[g]), int(bounds[g + 1])
+            s = self.streams[g % len(self.streams)]
+            s.wait_event(meta)
+            lo = int(off_np[a])
+            hi = int(off_np[b]) if deflate else int(off_np[b - 1] + len_np[b - 1])
+            hi = min(max(hi, lo), h_comp.numel())
+            ob = min(out_bytes, b * ch) - a * ch
+            with torch.cuda.stream(s):
+                if hi > lo:
+                    d_comp[lo:hi].copy_(h_comp[lo:hi], non_blocking=True)
+                sp = s.cuda_stream
+                if deflate:
+                    rc = lib.codag_decompress_deflate(d_comp.data_ptr(), h_comp.numel(), d_off.data_ptr() + 8 * a, b - a,
+                                                      ch, self.wrapper, d_out.data_ptr() + a * ch, max(ob, 0),
+                                                      d_st.data_ptr() + 4 * a, sp)
+                else:
+                    fn = lib.codag_decompress_rlev1 if self.codec == native.RLEV1 else lib.codag_decompress_rlev2
+                    rc = fn(d_comp.data_ptr(), h_comp.numel(), d_off.data_ptr() + 8 * a, d_len.data_ptr() + 8 * a,
+                            b - a, ch, self.elem, d_out.data_ptr() + a * ch, max(ob, 0), d_st.data_ptr() + 4 * a, None,
+                            0, sp)
+                check("HostPipeline decode", rc)
+                if ob > 0:
+                    h_out[a * ch:a * ch + ob].copy_(d_out[a * ch:a * ch + ob], non_blocking=True)
+        for s in self.streams:
+            main.wait_stream(s)
+        main.synchronize()
+        _status_error("HostPipeline", d_st[:n])
+
+
 # --- batched persistent plans --------------------------------------------------------------------
 class BatchPlan:
     """codag_batch_plan/run/destroy: one persistent launch over many independent chunks."""
