@@ -343,6 +343,120 @@ __device__ int decode_rlev1_chunk(InRing<NSLOT>& in, OUT& out, uint32_t cap) {
 }
 
 // RLE v2 (unsigned values, include/rlev2/decoder_new.h:909-1187)
+//
+// One header at pos, all lanes on the same data: expands it and advances pos and n.  Used
+// for headers the batched parse below does not size (a varint longer than its 16-byte look,
+// a malformed or truncated header).
+template <int NSLOT, int E, class OUT>
+__device__ __forceinline__ int rlev2_header(InRing<NSLOT>& in, OUT& out, uint32_t& pos, uint32_t& n, uint32_t cap,
+                                            uint32_t end, uint32_t lane) {
+  constexpr uint64_t M = emask<E>();
+  int st = in.advance(pos, min(pos + 32, end));
+  if (st) return st;
+  const uint64_t hdr = in.peek_be64(pos);
+  const uint32_t first = static_cast<uint32_t>(hdr >> 56);
+  // the length field is held in a uint8_t (decoder_new.h:1019,1048,1095)
+  const uint32_t len8 = ((static_cast<uint32_t>(hdr >> 48) & 0x1ffu) + 1u) & 0xffu;
+  uint32_t cnt, total;
+  if ((first >> 6) == 0) {  // SHORT_REPEAT (decoder_new.h:1004-1014)
+    const uint32_t nb = ((first >> 3) & 7u) + 1u;
+    cnt = (first & 7u) + 3u;
+    total = 1u + nb;
+    if (pos + total > end || n + cnt > cap) return CODAG_ECORRUPT;
+    const uint64_t v = nb < 8 ? (hdr << 8) >> (64u - 8u * nb) : in.peek_be64(pos + 1);
+    if (lane < cnt) put_elem<E>(out, n + lane, v & M);
+  } else if ((first >> 6) == 1) {  // DIRECT (decoder_new.h:1015-1043)
+    const uint32_t fbw = v2_width((first >> 1) & 0x1fu);
+    cnt = len8;
+    total = 2u + (len8 * fbw + 7u) / 8u;
+    if (pos + total > end || n + cnt > cap) return CODAG_ECORRUPT;
+    st = in.advance(pos, pos + total);
+    if (st) return st;
+    body_unpack<NSLOT, E>(in, out, n, cnt, (pos + 2u) * 8u, fbw, 0ull, lane);
+  } else if ((first >> 6) == 3) {  // DELTA (decoder_new.h:1044-1091)
+    const uint32_t enc = (first >> 1) & 0x1fu;
+    const uint32_t fbw = v2_width(enc);
+    uint32_t l1, l2;
+    uint64_t ub, ud;
+    if (!read_uvarint(in, pos + 2, end, l1, ub) || !read_uvarint(in, pos + 2 + l1, end, l2, ud)) {
+      return CODAG_ECORRUPT;
+    }
+    const uint64_t base = ub & M;
+    const int64_t sd = static_cast<int64_t>(ud);
+    const uint64_t bd = static_cast<uint64_t>((sd >> 1) ^ -(sd & 1)) & M;  // arithmetic shift (decoder_new.h:990)
+    const uint32_t nd = (len8 - 2u) & 0xffu;                              // "len -= 2" on a uint8_t
+    const uint32_t data = pos + 2u + l1 + l2;
+    cnt = nd + 2u;
+    total = (data - pos) + (enc ? (nd * fbw + 7u) / 8u : 0u);
+    if (pos + total > end || n + cnt > cap) return CODAG_ECORRUPT;
+    st = in.advance(pos, pos + total);
+    if (st) return st;
+    if (enc == 0) body_fill<E>(out, n, cnt, base, bd, lane);
+    else body_delta_packed<NSLOT, E>(in, out, n, nd, fbw, base, bd, data * 8u, lane);
+  } else {  // PATCHED_BASE (decoder_new.h:1092-1183)
+    const uint32_t fbw = v2_width((first >> 1) & 0x1fu);
+    const uint32_t third = static_cast<uint32_t>(hdr >> 40) & 0xffu;
+    const uint32_t fourth = static_cast<uint32_t>(hdr >> 32) & 0xffu;
+    const uint32_t bw = ((third >> 5) & 7u) + 1u;
+    const uint32_t pw = v2_width(third & 0x1fu);
+    const uint32_t pgw = ((fourth >> 5) & 7u) + 1u;
+    const uint32_t pll = fourth & 0x1fu;
+    if (pw + pgw > 64u) return CODAG_ECORRUPT;
+    const uint32_t cfb = v2_closest(pw + pgw);
+    const uint32_t vals = pos + 4u + bw;
+    const uint32_t patches = vals + (len8 * fbw + 7u) / 8u;
+    cnt = len8;
+    total = (patches - pos) + (pll * cfb + 7u) / 8u;
+    if (pos + total > end || n + cnt > cap) return CODAG_ECORRUPT;
+    st = in.advance(pos, pos + total);
+    if (st) return st;
+    const uint64_t base = in.peek_be64(pos + 4) >> (64u - 8u * bw);
+    body_unpack<NSLOT, E>(in, out, n, cnt, vals * 8u, fbw, base, lane);
+    if (pll) {
+      __syncwarp();
+      st = body_patches<NSLOT, E>(in, out, n, len8, fbw, pw, cfb, pll, base, patches * 8u, lane);
+      if (st) return st;
+    }
+  }
+  n += cnt;
+  pos += total;
+  out.flush_to(n * E);
+  return CODAG_OK;
+}
+
+// Byte size of the RLE v2 header at p from its leading bytes, or 0 when this look cannot
+// size it (DELTA varints not both inside the 8 bytes after the header, or a PATCHED_BASE
+// header whose patch width exceeds 64 bits).
+template <int NSLOT>
+__device__ __forceinline__ uint32_t rlev2_size(const InRing<NSLOT>& in, uint32_t p) {
+  const uint32_t w = __byte_perm(in.peek_le32(p), 0, 0x0123);  // bytes p..p+3, first byte on top
+  const uint32_t first = w >> 24;
+  const uint32_t len8 = (((w >> 16) & 0x1ffu) + 1u) & 0xffu;
+  const uint32_t fbw = v2_width((first >> 1) & 0x1fu);
+  switch (first >> 6) {
+    case 0: return 2u + ((first >> 3) & 7u);
+    case 1: return 2u + (len8 * fbw + 7u) / 8u;
+    case 3: {
+      const uint64_t t = ~in.peek_le64(p + 2) & 0x8080808080808080ull;
+      const uint64_t t2 = t & (t - 1ull);  // the second varint's last byte
+      if (!t2) return 0u;
+      const uint32_t nd = (len8 - 2u) & 0xffu;
+      return 2u + (ctz64(t2) >> 3) + 1u + (((first >> 1) & 0x1fu) ? (nd * fbw + 7u) / 8u : 0u);
+    }
+    default: {
+      const uint32_t third = (w >> 8) & 0xffu, fourth = w & 0xffu;
+      const uint32_t pw = v2_width(third & 0x1fu), pgw = ((fourth >> 5) & 7u) + 1u;
+      if (pw + pgw > 64u) return 0u;
+      return 4u + ((third >> 5) & 7u) + 1u + (len8 * fbw + 7u) / 8u + ((fourth & 0x1fu) * v2_closest(pw + pgw) + 7u) / 8u;
+    }
+  }
+}
+
+// Batched parse: the warp sizes up to 32 consecutive headers whose bytes are resident (a
+// short serial walk over their leading bytes), lane j then decodes header j's fields on
+// its own, and the headers are expanded in order with their fields taken from lane j by
+// shuffles.  Header decoding thus costs one lane-parallel pass per 32 headers instead of
+// a warp-uniform pass per header.
 template <int NSLOT, int E, class OUT>
 __device__ int decode_rlev2_chunk(InRing<NSLOT>& in, OUT& out, uint32_t cap) {
   constexpr uint64_t M = emask<E>();
@@ -352,78 +466,98 @@ __device__ int decode_rlev2_chunk(InRing<NSLOT>& in, OUT& out, uint32_t cap) {
   uint32_t n = 0;
   int st = CODAG_OK;
   while (pos < end) {
-    st = in.advance(pos, min(pos + 32, end));
-    if (st) break;
-    const uint64_t hdr = in.peek_be64(pos);
-    const uint32_t first = static_cast<uint32_t>(hdr >> 56);
-    // the length field is held in a uint8_t (decoder_new.h:1019,1048,1095)
-    const uint32_t len8 = ((static_cast<uint32_t>(hdr >> 48) & 0x1ffu) + 1u) & 0xffu;
-    uint32_t cnt, total;
-    if ((first >> 6) == 0) {  // SHORT_REPEAT (decoder_new.h:1004-1014)
-      const uint32_t nb = ((first >> 3) & 7u) + 1u;
-      cnt = (first & 7u) + 3u;
-      total = 1u + nb;
-      if (pos + total > end || n + cnt > cap) { st = CODAG_ECORRUPT; break; }
-      const uint64_t v = nb < 8 ? (hdr << 8) >> (64u - 8u * nb) : in.peek_be64(pos + 1);
-      if (lane < cnt) put_elem<E>(out, n + lane, v & M);
-    } else if ((first >> 6) == 1) {  // DIRECT (decoder_new.h:1015-1043)
-      const uint32_t fbw = v2_width((first >> 1) & 0x1fu);
-      cnt = len8;
-      total = 2u + (len8 * fbw + 7u) / 8u;
-      if (pos + total > end || n + cnt > cap) { st = CODAG_ECORRUPT; break; }
-      st = in.advance(pos, pos + total);
+    // the largest header spans 4 + 8 + 2040 + 248 bytes; make at least that much resident
+    if (pos >= in.release_at || min(pos + 2304u, end) > in.ready) {
+      st = in.advance(pos, min(pos + 2304u, end));
       if (st) break;
-      body_unpack<NSLOT, E>(in, out, n, cnt, (pos + 2u) * 8u, fbw, 0ull, lane);
-    } else if ((first >> 6) == 3) {  // DELTA (decoder_new.h:1044-1091)
-      const uint32_t enc = (first >> 1) & 0x1fu;
-      const uint32_t fbw = v2_width(enc);
-      uint32_t l1, l2;
-      uint64_t ub, ud;
-      if (!read_uvarint(in, pos + 2, end, l1, ub) || !read_uvarint(in, pos + 2 + l1, end, l2, ud)) {
-        st = CODAG_ECORRUPT;
-        break;
-      }
-      const uint64_t base = ub & M;
-      const int64_t sd = static_cast<int64_t>(ud);
-      const uint64_t bd = static_cast<uint64_t>((sd >> 1) ^ -(sd & 1)) & M;  // arithmetic shift (decoder_new.h:990)
-      const uint32_t nd = (len8 - 2u) & 0xffu;                              // "len -= 2" on a uint8_t
-      const uint32_t data = pos + 2u + l1 + l2;
-      cnt = nd + 2u;
-      total = (data - pos) + (enc ? (nd * fbw + 7u) / 8u : 0u);
-      if (pos + total > end || n + cnt > cap) { st = CODAG_ECORRUPT; break; }
-      st = in.advance(pos, pos + total);
-      if (st) break;
-      if (enc == 0) body_fill<E>(out, n, cnt, base, bd, lane);
-      else body_delta_packed<NSLOT, E>(in, out, n, nd, fbw, base, bd, data * 8u, lane);
-    } else {  // PATCHED_BASE (decoder_new.h:1092-1183)
-      const uint32_t fbw = v2_width((first >> 1) & 0x1fu);
-      const uint32_t third = static_cast<uint32_t>(hdr >> 40) & 0xffu;
-      const uint32_t fourth = static_cast<uint32_t>(hdr >> 32) & 0xffu;
-      const uint32_t bw = ((third >> 5) & 7u) + 1u;
-      const uint32_t pw = v2_width(third & 0x1fu);
-      const uint32_t pgw = ((fourth >> 5) & 7u) + 1u;
-      const uint32_t pll = fourth & 0x1fu;
-      if (pw + pgw > 64u) { st = CODAG_ECORRUPT; break; }
-      const uint32_t cfb = v2_closest(pw + pgw);
-      const uint32_t vals = pos + 4u + bw;
-      const uint32_t patches = vals + (len8 * fbw + 7u) / 8u;
-      cnt = len8;
-      total = (patches - pos) + (pll * cfb + 7u) / 8u;
-      if (pos + total > end || n + cnt > cap) { st = CODAG_ECORRUPT; break; }
-      st = in.advance(pos, pos + total);
-      if (st) break;
-      const uint64_t base = in.peek_be64(pos + 4) >> (64u - 8u * bw);
-      body_unpack<NSLOT, E>(in, out, n, cnt, vals * 8u, fbw, base, lane);
-      if (pll) {
-        __syncwarp();
-        st = body_patches<NSLOT, E>(in, out, n, len8, fbw, pw, cfb, pll, base, patches * 8u, lane);
-        if (st) break;
-      }
     }
-    n += cnt;
-    pos += total;
-    __syncwarp();
-    out.flush_to(n * E);
+    const uint32_t ready = in.ready;
+    const uint32_t lim = min(ready, end);
+    // 1. sizes of the next headers (warp-uniform walk over leading bytes only)
+    uint32_t k = 0, p = pos, mine = 0;
+    while (k < 32 && p < end && (p + 24u <= ready || ready >= end)) {
+      const uint32_t sz = rlev2_size(in, p);
+      if (!sz || p + sz > lim) break;
+      if (lane == k) mine = p;
+      p += sz;
+      k++;
+    }
+    if (k == 0) {  // not sizable here: the one-header path decodes it or reports the error
+      st = rlev2_header<NSLOT, E>(in, out, pos, n, cap, end, lane);
+      if (st) break;
+      continue;
+    }
+    // 2. lane j < k decodes header j
+    uint32_t kc = 0, bit = 0, pinfo = 0, pbit = 0;
+    uint64_t va = 0, vb = 0;
+    if (lane < k) {
+      const uint32_t w = __byte_perm(in.peek_le32(mine), 0, 0x0123);
+      const uint32_t first = w >> 24;
+      const uint32_t len8 = (((w >> 16) & 0x1ffu) + 1u) & 0xffu;
+      const uint32_t kind = first >> 6;
+      uint32_t cnt, fbw = v2_width((first >> 1) & 0x1fu);
+      if (kind == 0) {  // SHORT_REPEAT: big-endian value of nb bytes
+        const uint32_t nb = ((first >> 3) & 7u) + 1u;
+        cnt = (first & 7u) + 3u;
+        va = in.peek_be64(mine + 1) >> (64u - 8u * nb);
+      } else if (kind == 1) {  // DIRECT
+        cnt = len8;
+        bit = (mine + 2u) * 8u;
+      } else if (kind == 3) {  // DELTA: base and zigzag delta varints, both in these 8 bytes
+        const uint64_t lo = in.peek_le64(mine + 2);
+        const uint64_t t = ~lo & 0x8080808080808080ull;
+        const uint32_t l1 = (ctz64(t) >> 3) + 1u;
+        const uint32_t l12 = (ctz64(t & (t - 1ull)) >> 3) + 1u;
+        va = leb_compact(lo, l1) & M;
+        const int64_t sd = static_cast<int64_t>(leb_compact(lo >> (8u * l1), l12 - l1));
+        vb = static_cast<uint64_t>((sd >> 1) ^ -(sd & 1)) & M;  // arithmetic shift (decoder_new.h:990)
+        const uint32_t nd = (len8 - 2u) & 0xffu;                // "len -= 2" on a uint8_t
+        cnt = nd + 2u;
+        if (!((first >> 1) & 0x1fu)) fbw = 0;  // fixed delta
+        bit = (mine + 2u + l12) * 8u;
+      } else {  // PATCHED_BASE
+        const uint32_t third = (w >> 8) & 0xffu, fourth = w & 0xffu;
+        const uint32_t bw = ((third >> 5) & 7u) + 1u;
+        const uint32_t pw = v2_width(third & 0x1fu);
+        const uint32_t cfb = v2_closest(pw + ((fourth >> 5) & 7u) + 1u);
+        cnt = len8;
+        va = in.peek_be64(mine + 4) >> (64u - 8u * bw);
+        bit = (mine + 4u + bw) * 8u;
+        pbit = bit + ((len8 * fbw + 7u) / 8u) * 8u;
+        pinfo = pw | (cfb << 8) | ((fourth & 0x1fu) << 16);
+      }
+      kc = kind | (cnt << 2) | (fbw << 12);
+    }
+    // 3. expand the headers in order
+    for (uint32_t j = 0; j < k; j++) {
+      const uint32_t c = __shfl_sync(FULL, kc, j);
+      const uint32_t kind = c & 3u, cnt = (c >> 2) & 0x3ffu, fbw = c >> 12;
+      if (n + cnt > cap) { st = CODAG_ECORRUPT; break; }
+      if (kind == 0) {
+        const uint64_t v = shfl64(va, j);
+        if (lane < cnt) put_elem<E>(out, n + lane, v & M);
+      } else if (kind == 1) {
+        body_unpack<NSLOT, E>(in, out, n, cnt, __shfl_sync(FULL, bit, j), fbw, 0ull, lane);
+      } else if (kind == 3) {
+        const uint64_t base = shfl64(va, j), bd = shfl64(vb, j);
+        if (fbw == 0) body_fill<E>(out, n, cnt, base, bd, lane);
+        else body_delta_packed<NSLOT, E>(in, out, n, cnt - 2u, fbw, base, bd, __shfl_sync(FULL, bit, j), lane);
+      } else {
+        const uint64_t base = shfl64(va, j);
+        const uint32_t pi = __shfl_sync(FULL, pinfo, j);
+        body_unpack<NSLOT, E>(in, out, n, cnt, __shfl_sync(FULL, bit, j), fbw, base, lane);
+        if (pi >> 16) {
+          const uint32_t pb = __shfl_sync(FULL, pbit, j);
+          __syncwarp();
+          st = body_patches<NSLOT, E>(in, out, n, cnt, fbw, pi & 0xffu, (pi >> 8) & 0xffu, pi >> 16, base, pb, lane);
+          if (st) break;
+        }
+      }
+      n += cnt;
+      out.flush_to(n * E);
+    }
+    if (st) break;
+    pos = p;
   }
   if (!in.drain() && st == CODAG_OK) st = CODAG_ETIMEOUT;
   out.finish(n * E);
