@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <mutex>
 #include <new>
+#include <type_traits>
 #include <vector>
 
 #include "decode_deflate.cuh"
@@ -34,6 +35,14 @@ struct RleLayout {
   static constexpr uint32_t kIn = 0;
   static constexpr uint32_t kOut = kIn + NSLOT * kSlotBytes;
   static constexpr uint32_t kBar = kOut + RleOut::kBytes;
+  static constexpr uint32_t kPerWarp = align_up(kBar + NSLOT * 8, 128);
+};
+
+// RLE with DirectOut: no output ring
+template <int NSLOT>
+struct RleDirectLayout {
+  static constexpr uint32_t kIn = 0;
+  static constexpr uint32_t kBar = kIn + NSLOT * kSlotBytes;
   static constexpr uint32_t kPerWarp = align_up(kBar + NSLOT * 8, 128);
 };
 
@@ -80,7 +89,7 @@ __global__ void __launch_bounds__(128) k_rle_walk(const uint8_t* __restrict__ co
   counts[chunk] = k;
 }
 
-template <int NSLOT, int CODEC, int E>
+template <int NSLOT, int CODEC, int E, bool DIRECT>
 __global__ void __launch_bounds__(256) k_rle_plain(const uint8_t* __restrict__ comp, uint64_t comp_bytes,
                                                    const uint64_t* __restrict__ blk_off,
                                                    const uint64_t* __restrict__ col_len, uint64_t n_chunks,
@@ -89,7 +98,8 @@ __global__ void __launch_bounds__(256) k_rle_plain(const uint8_t* __restrict__ c
                                                    uint64_t wait_cycles, const uint32_t* __restrict__ counts,
                                                    const RleDesc* __restrict__ descs) {
   extern __shared__ __align__(128) uint8_t smem[];
-  using L = RleLayout<NSLOT>;
+  using L = std::conditional_t<DIRECT, RleDirectLayout<NSLOT>, RleLayout<NSLOT>>;
+  using OUT = std::conditional_t<DIRECT, DirectOut, RleOut>;
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint64_t chunk = static_cast<uint64_t>(blockIdx.x) * (blockDim.x >> 5) + warp;
   if (chunk >= n_chunks) return;
@@ -101,9 +111,11 @@ __global__ void __launch_bounds__(256) k_rle_plain(const uint8_t* __restrict__ c
   in.phase = 0;
   in.wait_cycles = wait_cycles;
   in.lane = lane;
-  RleOut o;
-  o.buf = base + L::kOut;
-  o.sbuf = smem_u32(o.buf);
+  OUT o;
+  if constexpr (!DIRECT) {
+    o.buf = base + L::kOut;
+    o.sbuf = smem_u32(o.buf);
+  }
   o.lane = lane;
   init_ring_barriers<NSLOT>(in.bar, lane);
 
@@ -244,6 +256,7 @@ __global__ void k_selftest_timeout(int32_t* status, uint64_t wait_cycles) {
 std::mutex g_mu;
 codag_tune g_tune[3] = {{8, 4, 10, 0}, {8, 4, 10, 0}, {2, 2, 9, 0}};
 uint64_t g_wait_cycles = 2000000000ull;  // about one second at 2 GHz
+bool g_direct_out = true;                 // RLE output path (see launch_rle)
 
 bool valid_slots(int s) { return s == 2 || s == 4 || s == 8; }
 bool valid_lut(int b) { return b == 9 || b == 10 || b == 11; }
@@ -273,13 +286,13 @@ codag_status finish_launch() {
 constexpr uint64_t rle_ws_counts_bytes(uint64_t n) { return (n * 4 + 255) / 256 * 256; }
 constexpr uint64_t rle_ws_bytes(uint64_t n) { return rle_ws_counts_bytes(n) + n * kDescPerChunk * sizeof(RleDesc); }
 
-template <int NSLOT, int CODEC, int E>
-codag_status launch_rle(const codag_tune& t, const uint8_t* comp, uint64_t comp_bytes, const uint64_t* blk_off,
-                        const uint64_t* col_len, uint64_t n, uint64_t chunk_bytes, uint8_t* out, uint64_t out_bytes,
-                        int32_t* status, void* ws, uint64_t ws_bytes, cudaStream_t s) {
-  using L = RleLayout<NSLOT>;
+template <int NSLOT, int CODEC, int E, bool DIRECT>
+codag_status launch_rle_out(const codag_tune& t, const uint8_t* comp, uint64_t comp_bytes, const uint64_t* blk_off,
+                            const uint64_t* col_len, uint64_t n, uint64_t chunk_bytes, uint8_t* out,
+                            uint64_t out_bytes, int32_t* status, void* ws, uint64_t ws_bytes, cudaStream_t s) {
+  using L = std::conditional_t<DIRECT, RleDirectLayout<NSLOT>, RleLayout<NSLOT>>;
   const uint32_t smem = L::kPerWarp * t.warps_per_cta;
-  auto kern = k_rle_plain<NSLOT, CODEC, E>;
+  auto kern = k_rle_plain<NSLOT, CODEC, E, DIRECT>;
   if (allow_smem(kern, smem) != cudaSuccess) return CODAG_ECUDA;
   const uint64_t grid = (n + t.warps_per_cta - 1) / t.warps_per_cta;
   if (grid > 0x7fffffffull) return CODAG_EINVAL;
@@ -295,6 +308,19 @@ codag_status launch_rle(const codag_tune& t, const uint8_t* comp, uint64_t comp_
                                                                          chunk_bytes, out, out_bytes, status,
                                                                          wait_of(), counts, descs);
   return finish_launch();
+}
+
+// Values go straight to global memory when the output is element aligned (DirectOut),
+// through the shared-memory ring otherwise.
+template <int NSLOT, int CODEC, int E>
+codag_status launch_rle(const codag_tune& t, const uint8_t* comp, uint64_t comp_bytes, const uint64_t* blk_off,
+                        const uint64_t* col_len, uint64_t n, uint64_t chunk_bytes, uint8_t* out, uint64_t out_bytes,
+                        int32_t* status, void* ws, uint64_t ws_bytes, cudaStream_t s) {
+  if ((reinterpret_cast<uintptr_t>(out) % E) == 0 && g_direct_out)
+    return launch_rle_out<NSLOT, CODEC, E, true>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, out,
+                                                 out_bytes, status, ws, ws_bytes, s);
+  return launch_rle_out<NSLOT, CODEC, E, false>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, out, out_bytes,
+                                                status, ws, ws_bytes, s);
 }
 
 template <int NSLOT, int CODEC>

@@ -19,7 +19,9 @@
 //   - RLE v2 packed DELTA: deltas unpacked per lane and accumulated with a warp scan;
 //   - PATCHED_BASE patches: gaps prefix-summed across the patch lanes, patches applied by
 //     those lanes (a group hitting one value is OR-combined first).
-// Values go to the shared-memory output ring (OutRing) and leave it as 16-byte stores.
+// Values go either to the shared-memory output ring (OutRing, drained by TMA bulk stores) or,
+// when the output is element aligned, straight to global memory (DirectOut), 32 consecutive
+// elements per warp store.
 // Element arithmetic is modulo 2^(8*E), keeping the reference's quirks (oracle/oracle.c).
 #pragma once
 #include "device_common.cuh"
@@ -44,20 +46,12 @@ __device__ __forceinline__ constexpr uint64_t emask() {
 
 template <int E, class OUT>
 __device__ __forceinline__ void put_elem(OUT& o, uint32_t idx, uint64_t v) {
-  const uint32_t a = o.sbuf + ((idx * static_cast<uint32_t>(E)) & OUT::kMask);
-  if constexpr (E == 8) st_s64(a, v);
-  else if constexpr (E == 4) st_s32(a, static_cast<uint32_t>(v));
-  else if constexpr (E == 2) st_s16(a, static_cast<uint32_t>(v));
-  else st_s8(a, static_cast<uint32_t>(v));
+  o.template put<E>(idx * static_cast<uint32_t>(E), v);
 }
 
 template <int E, class OUT>
 __device__ __forceinline__ uint64_t get_elem(const OUT& o, uint32_t idx) {
-  const uint32_t a = o.sbuf + ((idx * static_cast<uint32_t>(E)) & OUT::kMask);
-  if constexpr (E == 8) return ld_s64(a);
-  else if constexpr (E == 4) return ld_s32(a);
-  else if constexpr (E == 2) return ld_s16(a);
-  else return ld_s8(a);
+  return o.template get<E>(idx * static_cast<uint32_t>(E));
 }
 
 // bit width of a 5-bit width code (include/rlev2/utils.h:28)
@@ -136,15 +130,6 @@ __device__ __forceinline__ bool read_uvarint(InRing<NSLOT>& in, uint32_t p, uint
 // ---------------------------------------------------------------------------------------
 // per-header value expansion (warp-cooperative; all lanes call with identical arguments)
 // ---------------------------------------------------------------------------------------
-// store v (E bytes) at shared address a
-template <int E>
-__device__ __forceinline__ void st_elem(uint32_t a, uint64_t v) {
-  if constexpr (E == 8) st_s64(a, v);
-  else if constexpr (E == 4) st_s32(a, static_cast<uint32_t>(v));
-  else if constexpr (E == 2) st_s16(a, static_cast<uint32_t>(v));
-  else st_s8(a, static_cast<uint32_t>(v));
-}
-
 // value i = v + i*step, i < cnt
 template <int E, class OUT>
 __device__ __forceinline__ void body_fill(OUT& out, uint32_t n, uint32_t cnt, uint64_t v, uint64_t step, uint32_t lane) {
@@ -152,8 +137,7 @@ __device__ __forceinline__ void body_fill(OUT& out, uint32_t n, uint32_t cnt, ui
   uint64_t x = v + static_cast<uint64_t>(lane) * step;
   const uint64_t s32 = step << 5;
   uint32_t oa = (n + lane) * E;
-  const uint32_t base = out.sbuf;
-  for (uint32_t i = lane; i < cnt; i += 32, x += s32, oa += 32 * E) st_elem<E>(base + (oa & OUT::kMask), x);
+  for (uint32_t i = lane; i < cnt; i += 32, x += s32, oa += 32 * E) out.template put<E>(oa, x);
 }
 
 // value i = (fbw-bit field i at bit0, most significant bit first) + add, i < cnt
@@ -162,7 +146,7 @@ __device__ __forceinline__ void body_unpack(const InRing<NSLOT>& in, OUT& out, u
                                             uint32_t fbw, uint64_t add, uint32_t lane) {
   if (lane >= cnt) return;
   constexpr uint32_t IM = InRing<NSLOT>::kMask;
-  const uint32_t ib = in.sbuf, ob = out.sbuf;
+  const uint32_t ib = in.sbuf;
   uint32_t bp = bit0 + lane * fbw;
   const uint32_t bstep = fbw << 5;
   uint32_t oa = (n + lane) * E;
@@ -173,7 +157,7 @@ __device__ __forceinline__ void body_unpack(const InRing<NSLOT>& in, OUT& out, u
       const uint32_t w0 = __byte_perm(ld_s32(ib + (wa & IM)), 0, 0x0123);
       const uint32_t w1 = __byte_perm(ld_s32(ib + ((wa + 4) & IM)), 0, 0x0123);
       const uint32_t v = __funnelshift_l(w1, w0, bp & 31u) >> rs;
-      st_elem<E>(ob + (oa & OUT::kMask), static_cast<uint64_t>(v) + add);
+      out.template put<E>(oa, static_cast<uint64_t>(v) + add);
     }
   } else {
     const uint32_t rs = 64u - fbw;
@@ -183,7 +167,7 @@ __device__ __forceinline__ void body_unpack(const InRing<NSLOT>& in, OUT& out, u
       const uint32_t w1 = __byte_perm(ld_s32(ib + ((wa + 4) & IM)), 0, 0x0123);
       const uint32_t w2 = __byte_perm(ld_s32(ib + ((wa + 8) & IM)), 0, 0x0123);
       const uint64_t v = ((static_cast<uint64_t>(__funnelshift_l(w1, w0, s)) << 32) | __funnelshift_l(w2, w1, s)) >> rs;
-      st_elem<E>(ob + (oa & OUT::kMask), v + add);
+      out.template put<E>(oa, v + add);
     }
   }
 }

@@ -439,6 +439,63 @@ struct OutRing {
   // byte at stream position p of the window
   __device__ __forceinline__ uint32_t get8(uint32_t p) const { return ld_s8(sbuf + (p & kMask)); }
   __device__ __forceinline__ void put8(uint32_t p, uint32_t v) { st_s8(sbuf + (p & kMask), v); }
+
+  // E-byte element at byte offset `off` of the chunk (a stream position of the window)
+  template <int E>
+  __device__ __forceinline__ void put(uint32_t off, uint64_t v) {
+    const uint32_t a = sbuf + (off & kMask);
+    if constexpr (E == 8) st_s64(a, v);
+    else if constexpr (E == 4) st_s32(a, static_cast<uint32_t>(v));
+    else if constexpr (E == 2) st_s16(a, static_cast<uint32_t>(v));
+    else st_s8(a, static_cast<uint32_t>(v));
+  }
+  template <int E>
+  __device__ __forceinline__ uint64_t get(uint32_t off) const {
+    const uint32_t a = sbuf + (off & kMask);
+    if constexpr (E == 8) return ld_s64(a);
+    else if constexpr (E == 4) return ld_s32(a);
+    else if constexpr (E == 2) return ld_s16(a);
+    else return ld_s8(a);
+  }
+};
+
+// Output straight to global memory: lane i of a warp store writes element n + i, so one warp
+// store covers 32 consecutive elements (256 bytes for 8-byte values).  Needs the chunk's
+// output base aligned to the element width; elements at or beyond `store` are not written.
+// No staging, so nothing to drain.
+struct DirectOut {
+  static constexpr uint32_t kFlush = 0xffffffffu;
+  uint8_t* gdst;   // chunk output base (element aligned)
+  uint32_t store;  // bytes of this chunk that may be stored
+  uint32_t flushed;
+  uint32_t lane;
+
+  __device__ __forceinline__ void begin(uint8_t* dst, uint64_t store_bytes) {
+    gdst = dst;
+    store = static_cast<uint32_t>(store_bytes);
+    flushed = 0;
+  }
+  __device__ __forceinline__ void flush_to(uint32_t) {}
+  __device__ __forceinline__ void finish(uint32_t pos) { flushed = pos; }
+
+  template <int E>
+  __device__ __forceinline__ void put(uint32_t off, uint64_t v) {
+    if (off >= store) return;
+    uint8_t* a = gdst + off;
+    if constexpr (E == 8) *reinterpret_cast<uint64_t*>(a) = v;
+    else if constexpr (E == 4) *reinterpret_cast<uint32_t*>(a) = static_cast<uint32_t>(v);
+    else if constexpr (E == 2) *reinterpret_cast<uint16_t*>(a) = static_cast<uint16_t>(v);
+    else *a = static_cast<uint8_t>(v);
+  }
+  template <int E>
+  __device__ __forceinline__ uint64_t get(uint32_t off) const {
+    if (off >= store) return 0;  // never stored: the patch result is dropped as well
+    const uint8_t* a = gdst + off;
+    if constexpr (E == 8) return *reinterpret_cast<const uint64_t*>(a);
+    else if constexpr (E == 4) return *reinterpret_cast<const uint32_t*>(a);
+    else if constexpr (E == 2) return *reinterpret_cast<const uint16_t*>(a);
+    else return *a;
+  }
 };
 
 }  // namespace codag_dev

@@ -22,16 +22,19 @@ def _t(cuda, a, dtype=None):
     return cuda.from_numpy(a).to("cuda")
 
 
-def _gpu_rle(cuda, api, codec, comp, off, ln, chunk, e, out_bytes=None, comp_shift=0, two_pass=True):
+def _gpu_rle(cuda, api, codec, comp, off, ln, chunk, e, out_bytes=None, comp_shift=0, two_pass=True, out_shift=0):
     """Decode n RLE chunks on the GPU; comp_shift moves the whole stream buffer off 16-byte alignment;
-    two_pass=False decodes without a workspace (the warp walks the headers itself)."""
+    two_pass=False decodes without a workspace (the warp walks the headers itself); out_shift
+    moves the output off element alignment, which routes the values through the shared-memory
+    output ring instead of straight to global memory."""
     n = ln.size
     buf = np.zeros(comp.size + comp_shift, np.uint8)
     buf[comp_shift:] = comp
     d_buf = _t(cuda, buf)
     d_comp = d_buf[comp_shift:]
     total = n * chunk if out_bytes is None else out_bytes
-    out = cuda.full((total + 64,), 0xA5, dtype=cuda.uint8, device="cuda")
+    out_all = cuda.full((total + 64 + out_shift,), 0xA5, dtype=cuda.uint8, device="cuda")
+    out = out_all[out_shift:]
     st = cuda.full((n,), -1, dtype=cuda.int32, device="cuda")
     fn = api.decompress_rlev1 if codec == RLEV1 else api.decompress_rlev2
     kw = {"ws": api.AUTO_WORKSPACE} if two_pass else {}
@@ -39,6 +42,7 @@ def _gpu_rle(cuda, api, codec, comp, off, ln, chunk, e, out_bytes=None, comp_shi
     cuda.cuda.synchronize()
     o = out.cpu().numpy()
     assert np.all(o[total:] == 0xA5), "wrote past out_bytes"
+    assert np.all(out_all.cpu().numpy()[:out_shift] == 0xA5), "wrote before the output"
     return st.cpu().numpy(), o[:total]
 
 
@@ -51,12 +55,13 @@ def api(native, cuda):
 # --- known-answer vectors --------------------------------------------------------------------
 @pytest.mark.parametrize("two_pass", [True, False])
 @pytest.mark.parametrize("name", sorted(VECTORS))
-def test_known_answer_vectors(cuda, api, name, two_pass):
+@pytest.mark.parametrize("out_shift", [0, 1])
+def test_known_answer_vectors(cuda, api, name, two_pass, out_shift):
     codec, e, stream, expected = VECTORS[name]
     want = _bytes_of(expected, e)
     s = np.array(stream, np.uint8)
     st, out = _gpu_rle(cuda, api, codec, s, np.array([0], np.uint64), np.array([s.size], np.uint64), want.size, e,
-                       two_pass=two_pass)
+                       two_pass=two_pass, out_shift=out_shift)
     assert st.tolist() == [0]
     assert np.array_equal(out, want)
 
@@ -65,7 +70,8 @@ def test_known_answer_vectors(cuda, api, name, two_pass):
 @pytest.mark.parametrize("two_pass", [True, False])
 @pytest.mark.parametrize("e", [1, 2, 4, 8])
 @pytest.mark.parametrize("codec", [RLEV1, RLEV2])
-def test_rle_parity(native, oracle, cuda, api, codec, e, two_pass):
+@pytest.mark.parametrize("out_shift", [0, 1])
+def test_rle_parity(native, oracle, cuda, api, codec, e, two_pass, out_shift):
     n = (4 << 20) // e
     if codec == RLEV1:
         col = native.gen_rlev1_column(n, 31 + e, e)
@@ -75,7 +81,7 @@ def test_rle_parity(native, oracle, cuda, api, codec, e, two_pass):
         col = native.gen_rlev2_column(n, 37 + e, e)
         comp, off, ln = native.encode_rlev2(col, CH, e)
     nch = ln.size
-    st, out = _gpu_rle(cuda, api, codec, comp, off, ln, CH, e, two_pass=two_pass)
+    st, out = _gpu_rle(cuda, api, codec, comp, off, ln, CH, e, two_pass=two_pass, out_shift=out_shift)
     assert not st.any()
     assert np.array_equal(out[:col.size], col)
     ref = np.zeros(nch * CH, np.uint8)
