@@ -316,7 +316,8 @@ template <int NSLOT, int CODEC, int E>
 codag_status launch_rle(const codag_tune& t, const uint8_t* comp, uint64_t comp_bytes, const uint64_t* blk_off,
                         const uint64_t* col_len, uint64_t n, uint64_t chunk_bytes, uint8_t* out, uint64_t out_bytes,
                         int32_t* status, void* ws, uint64_t ws_bytes, cudaStream_t s) {
-  if ((reinterpret_cast<uintptr_t>(out) % E) == 0 && g_direct_out)
+  // direct stores write whole elements: the output and out_bytes must be element aligned
+  if ((reinterpret_cast<uintptr_t>(out) % E) == 0 && out_bytes % E == 0 && g_direct_out)
     return launch_rle_out<NSLOT, CODEC, E, true>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, out,
                                                  out_bytes, status, ws, ws_bytes, s);
   return launch_rle_out<NSLOT, CODEC, E, false>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, out, out_bytes,

@@ -136,8 +136,15 @@ __device__ __forceinline__ void body_fill(OUT& out, uint32_t n, uint32_t cnt, ui
   if (lane >= cnt) return;
   uint64_t x = v + static_cast<uint64_t>(lane) * step;
   const uint64_t s32 = step << 5;
-  uint32_t oa = (n + lane) * E;
-  for (uint32_t i = lane; i < cnt; i += 32, x += s32, oa += 32 * E) out.template put<E>(oa, x);
+  if constexpr (OUT::kDirect) {  // bounds hoisted out of the loop, a running element pointer
+    using T = typename ElemType<E>::T;
+    const uint32_t lim = out.template storable<E>(n, cnt);
+    T* dst = reinterpret_cast<T*>(out.gdst) + n + lane;
+    for (uint32_t i = lane; i < lim; i += 32, x += s32, dst += 32) *dst = static_cast<T>(x);
+  } else {
+    uint32_t oa = (n + lane) * E;
+    for (uint32_t i = lane; i < cnt; i += 32, x += s32, oa += 32 * E) out.template put<E>(oa, x);
+  }
 }
 
 // value i = (fbw-bit field i at bit0, most significant bit first) + add, i < cnt
@@ -152,6 +159,19 @@ __device__ __forceinline__ void body_unpack(const InRing<NSLOT>& in, OUT& out, u
   uint32_t oa = (n + lane) * E;
   if (fbw <= 32) {
     const uint32_t rs = 32u - fbw;
+    if constexpr (OUT::kDirect) {  // bounds hoisted out of the loop, a running element pointer
+      using T = typename ElemType<E>::T;
+      const uint32_t lim = out.template storable<E>(n, cnt);
+      T* dst = reinterpret_cast<T*>(out.gdst) + n + lane;
+      for (uint32_t j = lane; j < lim; j += 32, bp += bstep, dst += 32) {
+        const uint32_t wa = (bp >> 3) & ~3u;
+        const uint32_t w0 = __byte_perm(ld_s32(ib + (wa & IM)), 0, 0x0123);
+        const uint32_t w1 = __byte_perm(ld_s32(ib + ((wa + 4) & IM)), 0, 0x0123);
+        const uint32_t v = __funnelshift_l(w1, w0, bp & 31u) >> rs;
+        *dst = static_cast<T>(static_cast<uint64_t>(v) + add);
+      }
+      return;
+    }
     for (uint32_t j = lane; j < cnt; j += 32, bp += bstep, oa += 32 * E) {
       const uint32_t wa = (bp >> 3) & ~3u;
       const uint32_t w0 = __byte_perm(ld_s32(ib + (wa & IM)), 0, 0x0123);

@@ -357,6 +357,7 @@ struct OutRing {
   static constexpr uint32_t kBytes = 1u << LOG2_BYTES;
   static constexpr uint32_t kMask = kBytes - 1;
   static constexpr uint32_t kFlush = 1u << LOG2_FLUSH;
+  static constexpr bool kDirect = false;
   // BULK: complete pieces leave by TMA bulk stores issued by lane 0; no decoder may read
   // the chunk's output back from global memory while the stores are in flight.  A piece
   // may be rewritten once the store of the piece after it has been issued (the stores are
@@ -465,6 +466,7 @@ struct OutRing {
 // No staging, so nothing to drain.
 struct DirectOut {
   static constexpr uint32_t kFlush = 0xffffffffu;
+  static constexpr bool kDirect = true;
   uint8_t* gdst;   // chunk output base (element aligned)
   uint32_t store;  // bytes of this chunk that may be stored
   uint32_t flushed;
@@ -477,6 +479,12 @@ struct DirectOut {
   }
   __device__ __forceinline__ void flush_to(uint32_t) {}
   __device__ __forceinline__ void finish(uint32_t pos) { flushed = pos; }
+  // how many of the cnt E-byte elements from element n may be stored (store is a multiple of E)
+  template <int E>
+  __device__ __forceinline__ uint32_t storable(uint32_t n, uint32_t cnt) const {
+    const uint32_t se = store / static_cast<uint32_t>(E);
+    return n >= se ? 0u : (cnt < se - n ? cnt : se - n);
+  }
 
   template <int E>
   __device__ __forceinline__ void put(uint32_t off, uint64_t v) {

@@ -104,6 +104,21 @@ def test_rle_exact_size_output_and_unaligned_base(native, cuda, api, codec):
     assert np.array_equal(out, col)
 
 
+@pytest.mark.parametrize("cut", [1, 3, 7])
+@pytest.mark.parametrize("codec", [RLEV1, RLEV2])
+def test_rle_output_size_not_a_multiple_of_the_element(native, cuda, api, codec, cut):
+    """out_bytes ending inside an 8-byte element: the bytes up to out_bytes are stored and
+    nothing after them (the helper checks the guard bytes)."""
+    col = (native.gen_rlev1_column if codec == RLEV1 else native.gen_rlev2_column)(300_000, 19, 8)
+    comp, off, ln = (native.encode_rlev1 if codec == RLEV1 else native.encode_rlev2)(col, CH, 8)
+    if codec == RLEV1:
+        comp = comp[8:]
+    size = col.size - cut
+    st, out = _gpu_rle(cuda, api, codec, comp, off, ln, CH, 8, out_bytes=size)
+    assert not st.any()
+    assert np.array_equal(out, col[:size])
+
+
 def test_rle_odd_chunk_sizes(native, oracle, cuda, api):
     """Chunk sizes that are not multiples of 16 take the unaligned drain path."""
     for chunk, e in ((4104, 8), (1000, 4), (998, 2), (777, 1)):
