@@ -256,7 +256,6 @@ __global__ void k_selftest_timeout(int32_t* status, uint64_t wait_cycles) {
 std::mutex g_mu;
 codag_tune g_tune[3] = {{8, 4, 10, 0}, {8, 4, 10, 0}, {2, 2, 9, 0}};
 uint64_t g_wait_cycles = 2000000000ull;  // about one second at 2 GHz
-bool g_direct_out = true;                 // RLE output path (see launch_rle)
 
 bool valid_slots(int s) { return s == 2 || s == 4 || s == 8; }
 bool valid_lut(int b) { return b == 9 || b == 10 || b == 11; }
@@ -317,7 +316,7 @@ codag_status launch_rle(const codag_tune& t, const uint8_t* comp, uint64_t comp_
                         const uint64_t* col_len, uint64_t n, uint64_t chunk_bytes, uint8_t* out, uint64_t out_bytes,
                         int32_t* status, void* ws, uint64_t ws_bytes, cudaStream_t s) {
   // direct stores write whole elements: the output and out_bytes must be element aligned
-  if ((reinterpret_cast<uintptr_t>(out) % E) == 0 && out_bytes % E == 0 && g_direct_out)
+  if ((reinterpret_cast<uintptr_t>(out) % E) == 0 && out_bytes % E == 0)
     return launch_rle_out<NSLOT, CODEC, E, true>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, out,
                                                  out_bytes, status, ws, ws_bytes, s);
   return launch_rle_out<NSLOT, CODEC, E, false>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, out, out_bytes,
