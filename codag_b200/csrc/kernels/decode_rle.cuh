@@ -140,6 +140,7 @@ __device__ __forceinline__ void body_fill(OUT& out, uint32_t n, uint32_t cnt, ui
     using T = typename ElemType<E>::T;
     const uint32_t lim = out.template storable<E>(n, cnt);
     T* dst = reinterpret_cast<T*>(out.gdst) + n + lane;
+#pragma unroll 4  // independent iterations: unrolled they overlap their latencies
     for (uint32_t i = lane; i < lim; i += 32, x += s32, dst += 32) *dst = static_cast<T>(x);
   } else {
     uint32_t oa = (n + lane) * E;
@@ -163,6 +164,7 @@ __device__ __forceinline__ void body_unpack(const InRing<NSLOT>& in, OUT& out, u
       using T = typename ElemType<E>::T;
       const uint32_t lim = out.template storable<E>(n, cnt);
       T* dst = reinterpret_cast<T*>(out.gdst) + n + lane;
+#pragma unroll 4
       for (uint32_t j = lane; j < lim; j += 32, bp += bstep, dst += 32) {
         const uint32_t wa = (bp >> 3) & ~3u;
         const uint32_t w0 = __byte_perm(ld_s32(ib + (wa & IM)), 0, 0x0123);
@@ -181,6 +183,21 @@ __device__ __forceinline__ void body_unpack(const InRing<NSLOT>& in, OUT& out, u
     }
   } else {
     const uint32_t rs = 64u - fbw;
+    if constexpr (OUT::kDirect) {
+      using T = typename ElemType<E>::T;
+      const uint32_t lim = out.template storable<E>(n, cnt);
+      T* dst = reinterpret_cast<T*>(out.gdst) + n + lane;
+#pragma unroll 4
+      for (uint32_t j = lane; j < lim; j += 32, bp += bstep, dst += 32) {
+        const uint32_t wa = (bp >> 3) & ~3u, s = bp & 31u;
+        const uint32_t w0 = __byte_perm(ld_s32(ib + (wa & IM)), 0, 0x0123);
+        const uint32_t w1 = __byte_perm(ld_s32(ib + ((wa + 4) & IM)), 0, 0x0123);
+        const uint32_t w2 = __byte_perm(ld_s32(ib + ((wa + 8) & IM)), 0, 0x0123);
+        const uint64_t v = ((static_cast<uint64_t>(__funnelshift_l(w1, w0, s)) << 32) | __funnelshift_l(w2, w1, s)) >> rs;
+        *dst = static_cast<T>(v + add);
+      }
+      return;
+    }
     for (uint32_t j = lane; j < cnt; j += 32, bp += bstep, oa += 32 * E) {
       const uint32_t wa = (bp >> 3) & ~3u, s = bp & 31u;
       const uint32_t w0 = __byte_perm(ld_s32(ib + (wa & IM)), 0, 0x0123);
