@@ -222,7 +222,9 @@ def run_ours(args, rank: int, world: int, local: int):
         nat.set_tune(codec, *[int(x) for x in args.tune.split(",")])
     elif args.autotune:
         from codag_b200 import tuning
-        best, res = tuning.autotune(codec, launch, use_cache=args.autotune == "cached", verbose=rank == 0)
+        # the best shape depends on the chunk count (few chunks favour a CTA per chunk)
+        best, res = tuning.autotune(codec, launch, tag=f"plain-{n}chunks", use_cache=args.autotune == "cached",
+                                    verbose=rank == 0)
     for _ in range(max(args.warmup, 3)):
         launch()
     torch.cuda.synchronize()
@@ -308,7 +310,8 @@ def run_ours(args, rank: int, world: int, local: int):
                    "chunk_bytes": CH, "n_chunks": n, "comp_bytes": comp_bytes,
                    "out_bytes": out_bytes, "l2": "inputs larger than L2 (no flush)",
                    "parallelism": f"{world} GPU(s), chunks per GPU independent",
-                   "tune": {k: getattr(nat.get_tune(codec), k) for k in ("warps_per_cta", "ring_slots", "lut_bits")}},
+                   "tune": {k: getattr(nat.get_tune(codec), k)
+                            for k in ("warps_per_cta", "ring_slots", "lut_bits", "cta_per_chunk")}},
         "bit_exact": ok,
         "e2e": {"value": round(world * out_bytes * e_steps / e2e_t / 1e9, 2), "unit": "GB/s",
                 "h2d_bytes_per_step": int(h2d_bytes), "d2h_bytes_per_step": int(out_bytes)},
@@ -336,7 +339,7 @@ def main():
                     help="pick the launch shape with the autotuner (cached result or a fresh search)")
     ap.add_argument("--rle-passes", type=int, default=1, choices=[1, 2],
                     help="RLE: 2 = header walk + expansion (with workspace), 1 = single pass")
-    ap.add_argument("--tune", default="", help="explicit launch shape warps_per_cta,ring_slots,lut_bits")
+    ap.add_argument("--tune", default="", help="explicit launch shape warps_per_cta,ring_slots,lut_bits[,cta_per_chunk]")
     ap.add_argument("--n-values", type=int, default=None,
                     help="override the workload's element count (profiling cases; not a bench line)")
     ap.add_argument("--n-files", type=int, default=None, help="batched: number of files (default 20,000)")

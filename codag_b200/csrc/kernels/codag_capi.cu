@@ -231,6 +231,146 @@ __global__ void __launch_bounds__(256) k_batch(const codag_chunk_desc* __restric
   }
 }
 
+// ---------------------------------------------------------------------------------------
+// one CTA per chunk (RLE, values straight to global memory)
+// ---------------------------------------------------------------------------------------
+// The CTA copies the whole stream into shared memory, warp 0 walks the headers into
+// shared-memory descriptors (with each header's first value index), and every warp expands
+// an equal share of the descriptors.  A stream larger than the staging buffer, or one whose
+// walk gives up (malformed, more headers than the descriptor budget), is decoded by warp 0
+// in one pass with the usual TMA ring, which reports the exact error.
+constexpr uint32_t kStageBytes = 64u << 10;
+constexpr int kStageSlots = static_cast<int>(kStageBytes >> kSlotLog2);
+struct CtaLayout {
+  static constexpr uint32_t kStage = 0;
+  static constexpr uint32_t kDesc = kStage + kStageBytes;
+  static constexpr uint32_t kNStart = kDesc + kDescPerChunk * sizeof(RleDesc);
+  static constexpr uint32_t kBar = kNStart + kDescPerChunk * 4;
+  static constexpr uint32_t kMisc = kBar + 64;
+  static constexpr uint32_t kBytes = kMisc + 64;
+};
+
+template <int CODEC, int E>
+__global__ void __launch_bounds__(256) k_rle_cta(const uint8_t* __restrict__ comp, uint64_t comp_bytes,
+                                                 const uint64_t* __restrict__ blk_off,
+                                                 const uint64_t* __restrict__ col_len, uint64_t n_chunks,
+                                                 uint64_t chunk_bytes, uint8_t* __restrict__ out, uint64_t out_bytes,
+                                                 int32_t* __restrict__ status, uint64_t wait_cycles) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  using L = CtaLayout;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const uint64_t chunk = blockIdx.x;
+  if (chunk >= n_chunks) return;
+  uint8_t* stage = smem + L::kStage;
+  RleDesc* desc = reinterpret_cast<RleDesc*>(smem + L::kDesc);
+  uint32_t* nstart = reinterpret_cast<uint32_t*>(smem + L::kNStart);
+  uint32_t* misc = reinterpret_cast<uint32_t*>(smem + L::kMisc);  // [0] descriptors, [1] status, [2] values
+  const uint64_t off = blk_off[chunk], len = col_len[chunk];
+  const uint64_t cbase = chunk * chunk_bytes;
+  const uint32_t cap = static_cast<uint32_t>(chunk_bytes / E);
+  const bool inb = stream_in_bounds(off, len, comp_bytes);
+  const uintptr_t a = reinterpret_cast<uintptr_t>(comp + off);
+  const uint8_t* g0 = reinterpret_cast<const uint8_t*>(a & ~static_cast<uintptr_t>(15));
+  const uint32_t lo = static_cast<uint32_t>(a & 15);
+  const uint32_t hi = inb ? lo + static_cast<uint32_t>(len) : 0u;
+  const bool staged = inb && hi <= kStageBytes;
+  if (threadIdx.x == 0) {
+    misc[0] = kWalkFallback;
+    misc[1] = CODAG_OK;
+    misc[2] = 0;
+  }
+  if (staged) {  // 16-byte granules covering [lo, hi); bytes outside the buffer read as 0
+    const uint8_t* end = comp + comp_bytes;
+    for (uint32_t g = threadIdx.x; g < (hi + 15u) >> 4; g += blockDim.x) {
+      const uint8_t* q = g0 + 16u * g;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (q >= comp && q + 16 <= end) {
+        v = __ldg(reinterpret_cast<const uint4*>(q));
+      } else {
+        uint32_t w[4] = {0, 0, 0, 0};
+        for (int i = 0; i < 16; i++)
+          if (q + i >= comp && q + i < end) w[i >> 2] |= static_cast<uint32_t>(__ldg(q + i)) << (8 * (i & 3));
+        v = make_uint4(w[0], w[1], w[2], w[3]);
+      }
+      *reinterpret_cast<uint4*>(stage + 16u * g) = v;
+    }
+  }
+  fence_proxy_async_smem();  // the one-pass fallback may refill the stage by TMA
+  // a fully resident view of the stage (every slot counted as arrived, nothing to release)
+  InRing<kStageSlots> in;
+  in.buf = stage;
+  in.sbuf = smem_u32(stage);
+  in.bar = nullptr;
+  in.gbase = g0;
+  in.lo = lo;
+  in.hi = hi;
+  in.nslots = (hi + kSlotBytes - 1) >> kSlotLog2;
+  in.issued = in.waited = in.nslots;
+  in.ready = in.nslots << kSlotLog2;
+  in.release_at = 0xffffffffu;
+  in.phase = 0;
+  in.wait_cycles = wait_cycles;
+  in.lane = lane;
+  __syncthreads();
+  if (staged && warp == 0) {  // RLE v1: the whole warp walks; RLE v2: one thread
+    uint32_t k;
+    if constexpr (CODEC == CODAG_CODEC_RLEV1) {
+      k = walk_rlev1_warp(in, static_cast<uint32_t>(len), cap, desc, nstart, lane);
+    } else {
+      k = 0;
+      if (lane == 0) {
+        const SStream sv{smem_u32(stage), lo, static_cast<uint32_t>(len), kStageBytes - 1u};
+        k = walk_rlev2(sv, cap, desc, nstart);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) {
+      misc[0] = k;
+      if (k != kWalkFallback && k) misc[2] = nstart[k - 1] + ((desc[k - 1].info >> 7) & 0x1ffu);
+    }
+  }
+  __syncthreads();
+  const uint32_t nd = misc[0];
+  DirectOut o;
+  o.lane = lane;
+  if (nd == kWalkFallback) {
+    if (warp == 0) {  // one pass through a TMA ring in the (unused) staging buffer
+      InRing<4> ring;
+      ring.buf = stage;
+      ring.sbuf = smem_u32(stage);
+      ring.bar = reinterpret_cast<uint64_t*>(smem + L::kBar);
+      ring.phase = 0;
+      ring.wait_cycles = wait_cycles;
+      ring.lane = lane;
+      init_ring_barriers<4>(ring.bar, lane);
+      int st = CODAG_ECORRUPT;
+      if (inb) {
+        ring.begin(comp + off, static_cast<uint32_t>(len));
+        o.begin(out + cbase, store_bytes(cbase, chunk_bytes, out_bytes));
+        st = CODEC == CODAG_CODEC_RLEV1 ? decode_rlev1_chunk<4, E>(ring, o, cap) : decode_rlev2_chunk<4, E>(ring, o, cap);
+      }
+      if (status && lane == 0) status[chunk] = st;
+    }
+    return;
+  }
+  // every warp expands descriptors [k0, k1)
+  o.begin(out + cbase, store_bytes(cbase, chunk_bytes, out_bytes));
+  const uint32_t k0 = static_cast<uint32_t>((static_cast<uint64_t>(nd) * warp) / nw);
+  const uint32_t k1 = static_cast<uint32_t>((static_cast<uint64_t>(nd) * (warp + 1)) / nw);
+  if (k0 < k1) {
+    uint32_t n = nstart[k0];
+    const int st = CODEC == CODAG_CODEC_RLEV1 ? expand_rlev1_range<kStageSlots, E, true>(in, o, desc, k0, k1, n)
+                                              : expand_rlev2_range<kStageSlots, E, true>(in, o, desc, k0, k1, n);
+    if (st && lane == 0) atomicMax(&misc[1], static_cast<uint32_t>(st));
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && status) {
+    int st = static_cast<int>(misc[1]);
+    if (st == CODAG_OK && static_cast<uint64_t>(misc[2]) * E < o.store) st = CODAG_ECORRUPT;
+    status[chunk] = st;
+  }
+}
+
 // A wait that no copy ever completes: exercises the bounded-wait path of InRing.
 __global__ void k_selftest_timeout(int32_t* status, uint64_t wait_cycles) {
   __shared__ __align__(128) uint8_t buf[kSlotBytes];
@@ -309,14 +449,30 @@ codag_status launch_rle_out(const codag_tune& t, const uint8_t* comp, uint64_t c
   return finish_launch();
 }
 
+template <int CODEC, int E>
+codag_status launch_rle_cta(const codag_tune& t, const uint8_t* comp, uint64_t comp_bytes, const uint64_t* blk_off,
+                            const uint64_t* col_len, uint64_t n, uint64_t chunk_bytes, uint8_t* out,
+                            uint64_t out_bytes, int32_t* status, cudaStream_t s) {
+  auto kern = k_rle_cta<CODEC, E>;
+  if (allow_smem(kern, CtaLayout::kBytes) != cudaSuccess) return CODAG_ECUDA;
+  if (n > 0x7fffffffull) return CODAG_EINVAL;
+  kern<<<static_cast<unsigned>(n), 32 * t.warps_per_cta, CtaLayout::kBytes, s>>>(
+      comp, comp_bytes, blk_off, col_len, n, chunk_bytes, out, out_bytes, status, wait_of());
+  return finish_launch();
+}
+
 // Values go straight to global memory when the output is element aligned (DirectOut),
-// through the shared-memory ring otherwise.
+// through the shared-memory ring otherwise; with cta_per_chunk (and no workspace) a whole
+// CTA decodes each chunk.
 template <int NSLOT, int CODEC, int E>
 codag_status launch_rle(const codag_tune& t, const uint8_t* comp, uint64_t comp_bytes, const uint64_t* blk_off,
                         const uint64_t* col_len, uint64_t n, uint64_t chunk_bytes, uint8_t* out, uint64_t out_bytes,
                         int32_t* status, void* ws, uint64_t ws_bytes, cudaStream_t s) {
   // direct stores write whole elements: the output and out_bytes must be element aligned
-  if ((reinterpret_cast<uintptr_t>(out) % E) == 0 && out_bytes % E == 0)
+  const bool direct = (reinterpret_cast<uintptr_t>(out) % E) == 0 && out_bytes % E == 0;
+  if (direct && t.cta_per_chunk && !ws)
+    return launch_rle_cta<CODEC, E>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, out, out_bytes, status, s);
+  if (direct)
     return launch_rle_out<NSLOT, CODEC, E, true>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, out,
                                                  out_bytes, status, ws, ws_bytes, s);
   return launch_rle_out<NSLOT, CODEC, E, false>(t, comp, comp_bytes, blk_off, col_len, n, chunk_bytes, out, out_bytes,
@@ -478,6 +634,7 @@ extern "C" codag_status codag_set_tune(int codec, const codag_tune* tune) {
   // an RLE v2 header with its data spans up to 2060 bytes; it must fit the window of
   // (slots - 1) KiB ahead of the read position
   if (codec != CODAG_CODEC_DEFLATE && tune->ring_slots < 4) return CODAG_EINVAL;
+  if (tune->cta_per_chunk != 0 && (tune->cta_per_chunk != 1 || codec == CODAG_CODEC_DEFLATE)) return CODAG_EINVAL;
   std::lock_guard<std::mutex> g(g_mu);
   g_tune[codec] = *tune;
   return CODAG_OK;

@@ -64,6 +64,35 @@ struct GStream {
   }
 };
 
+// the same view of a stream staged whole in shared memory (stream byte 0 at sbuf + lo)
+struct SStream {
+  uint32_t sbuf;  // shared address of the staging buffer
+  uint32_t lo;    // offset of the stream's first byte in it
+  uint32_t len;
+  uint32_t mask;  // staging buffer bytes - 1 (a power of two)
+  __device__ __forceinline__ void peek16(uint32_t p, uint64_t& lo8, uint64_t& hi8) const {
+    const uint32_t a = lo + p;
+    const uint32_t w = a & ~3u, sh = (a & 3u) * 8u;
+    uint32_t x[5];
+#pragma unroll
+    for (int i = 0; i < 5; i++) x[i] = ld_s32(sbuf + ((w + 4u * i) & mask));
+    const uint32_t y0 = __funnelshift_r(x[0], x[1], sh), y1 = __funnelshift_r(x[1], x[2], sh);
+    const uint32_t y2 = __funnelshift_r(x[2], x[3], sh), y3 = __funnelshift_r(x[3], x[4], sh);
+    lo8 = (static_cast<uint64_t>(y1) << 32) | y0;
+    hi8 = (static_cast<uint64_t>(y3) << 32) | y2;
+    // bytes past the stream read as zero, as in GStream outside the buffer
+    if (p + 16u > len) {
+      const uint32_t valid = p >= len ? 0u : len - p;
+      if (valid < 8) {
+        lo8 &= valid ? ((1ull << (8 * valid)) - 1ull) : 0ull;
+        hi8 = 0;
+      } else {
+        hi8 &= valid == 8 ? 0ull : ((1ull << (8 * (valid - 8))) - 1ull);
+      }
+    }
+  }
+};
+
 __device__ __forceinline__ uint64_t be_bytes(uint64_t le, uint32_t nb) {  // first nb bytes, big-endian
   return bswap64(le) >> (64u - 8u * nb);
 }
@@ -71,10 +100,12 @@ __device__ __forceinline__ uint64_t be_bytes(uint64_t le, uint32_t nb) {  // fir
 // ---------------------------------------------------------------------------------------
 // walks (one thread per chunk); return the descriptor count or kWalkFallback
 // ---------------------------------------------------------------------------------------
-__device__ uint32_t walk_rlev2(const GStream& g, uint32_t cap, RleDesc* __restrict__ d) {
+template <class S>
+__device__ uint32_t walk_rlev2(const S& g, uint32_t cap, RleDesc* __restrict__ d, uint32_t* __restrict__ nstart = nullptr,
+                               uint32_t budget = kDescPerChunk) {
   uint32_t pos = 0, n = 0, k = 0;
   while (pos < g.len) {
-    if (k == kDescPerChunk) return kWalkFallback;
+    if (k == budget) return kWalkFallback;
     uint64_t lo8, hi8;
     g.peek16(pos, lo8, hi8);
     const uint32_t first = static_cast<uint32_t>(lo8 & 0xff);
@@ -124,6 +155,7 @@ __device__ uint32_t walk_rlev2(const GStream& g, uint32_t cap, RleDesc* __restri
     }
     if (pos + h.total > g.len || h.total > 3000u || n + cnt > cap) return kWalkFallback;
     h.info = kind | (code << 2) | (cnt << 7) | extra;
+    if (nstart) nstart[k] = n;
     d[k++] = h;
     pos += h.total;
     n += cnt;
@@ -132,7 +164,8 @@ __device__ uint32_t walk_rlev2(const GStream& g, uint32_t cap, RleDesc* __restri
 }
 
 // position just past the `cnt`-th varint end at or after p, or 0 if the stream ends first
-__device__ __forceinline__ uint32_t skip_varints(const GStream& g, uint32_t p, uint32_t cnt) {
+template <class S>
+__device__ __forceinline__ uint32_t skip_varints(const S& g, uint32_t p, uint32_t cnt) {
   while (p < g.len) {
     uint64_t lo8, hi8;
     g.peek16(p, lo8, hi8);
@@ -159,10 +192,12 @@ __device__ __forceinline__ uint32_t skip_varints(const GStream& g, uint32_t p, u
   return 0;
 }
 
-__device__ uint32_t walk_rlev1(const GStream& g, uint32_t cap, RleDesc* __restrict__ d) {
+template <class S>
+__device__ uint32_t walk_rlev1(const S& g, uint32_t cap, RleDesc* __restrict__ d, uint32_t* __restrict__ nstart = nullptr,
+                               uint32_t budget = kDescPerChunk) {
   uint32_t pos = 0, n = 0, k = 0;
   while (n < cap) {
-    if (k == kDescPerChunk || pos >= g.len) return kWalkFallback;
+    if (k == budget || pos >= g.len) return kWalkFallback;
     uint64_t lo8, hi8;
     g.peek16(pos, lo8, hi8);
     const int h = static_cast<int8_t>(lo8 & 0xff);
@@ -190,7 +225,81 @@ __device__ uint32_t walk_rlev1(const GStream& g, uint32_t cap, RleDesc* __restri
       r.info = 1u | (cnt << 7);
     }
     if (pos + r.total > g.len || n + cnt > cap) return kWalkFallback;
+    if (nstart) nstart[k] = n;
     d[k++] = r;
+    pos += r.total;
+    n += cnt;
+  }
+  return k;
+}
+
+// RLE v1 walk by a whole warp over a stream resident in `in` (stream byte 0 at in.lo): the
+// same descriptors as walk_rlev1, but literal groups are skipped 128 bytes per step (each
+// lane counts the varint ends in its 4 bytes, a warp scan finds the lane holding the end).
+template <int NSLOT>
+__device__ uint32_t walk_rlev1_warp(const InRing<NSLOT>& in, uint32_t len, uint32_t cap, RleDesc* __restrict__ d,
+                                    uint32_t* __restrict__ nstart, uint32_t lane) {
+  const uint32_t base = in.lo;
+  uint32_t pos = 0, n = 0, k = 0;
+  while (n < cap) {
+    if (k == kDescPerChunk || pos >= len) return kWalkFallback;
+    const uint64_t lo8 = in.peek_le64(base + pos), hi8 = in.peek_le64(base + pos + 8);
+    const int h = static_cast<int8_t>(lo8 & 0xff);
+    RleDesc r;
+    r.pos = pos;
+    uint32_t cnt;
+    if (h >= 0) {  // run
+      const uint64_t v_lo = (lo8 >> 16) | (hi8 << 48), v_hi = hi8 >> 16;
+      const uint32_t l = leb_len(v_lo, v_hi);
+      if (!l || l > 12) return kWalkFallback;
+      cnt = static_cast<uint32_t>(h) + 3u;
+      r.a = leb_value(v_lo, v_hi, l);
+      r.b = static_cast<uint64_t>(static_cast<int64_t>(static_cast<int8_t>((lo8 >> 8) & 0xff)));
+      r.data = pos + 2u;
+      r.total = 2u + l;
+      r.info = cnt << 7;
+    } else {  // literal group: find the end of its cnt varints
+      cnt = static_cast<uint32_t>(-h);
+      uint32_t p = pos + 1, rem = cnt, e = 0;
+      for (;;) {
+        if (p >= len) return kWalkFallback;
+        const uint32_t q0 = p + 4u * lane;
+        const uint32_t tb = ~in.peek_le32(base + q0) & 0x80808080u;
+        uint32_t nib = ((tb >> 7) & 1u) | ((tb >> 14) & 2u) | ((tb >> 21) & 4u) | ((tb >> 28) & 8u);
+        if (q0 + 4 > len) nib &= q0 >= len ? 0u : ((1u << (len - q0)) - 1u);
+        const uint32_t c = __popc(nib);
+        uint32_t incl = c;
+#pragma unroll
+        for (int dd = 1; dd < 32; dd <<= 1) {
+          const uint32_t o = __shfl_up_sync(FULL, incl, dd);
+          if (lane >= static_cast<uint32_t>(dd)) incl += o;
+        }
+        const uint32_t total = __shfl_sync(FULL, incl, 31);
+        if (total >= rem) {
+          uint32_t endp = 0;
+          if (incl >= rem && incl - c < rem) {  // this lane holds the rem-th end
+            uint32_t m = nib;
+            for (uint32_t t = rem - (incl - c); t > 1; t--) m &= m - 1;
+            endp = q0 + static_cast<uint32_t>(__ffs(m));  // one past the end byte
+          }
+          e = __reduce_max_sync(FULL, endp);
+          break;
+        }
+        rem -= total;
+        p += 128;
+      }
+      r.a = 0;
+      r.b = 0;
+      r.data = pos + 1u;
+      r.total = e - pos;
+      r.info = 1u | (cnt << 7);
+    }
+    if (pos + r.total > len || n + cnt > cap) return kWalkFallback;
+    if (lane == 0) {
+      nstart[k] = n;
+      d[k] = r;
+    }
+    k++;
     pos += r.total;
     n += cnt;
   }
@@ -202,31 +311,39 @@ __device__ uint32_t walk_rlev1(const GStream& g, uint32_t cap, RleDesc* __restri
 // ---------------------------------------------------------------------------------------
 struct DescCache {  // descriptors [base, base+32) spread over the lanes
   uint4 c0, c1;
+  // d in global memory (read-only path) or, with SMEM, in shared memory
+  template <bool SMEM = false>
   __device__ __forceinline__ void load(const RleDesc* __restrict__ d, uint32_t first, uint32_t nd, uint32_t lane) {
     const uint32_t k = first + lane;
     if (k < nd) {
       const uint4* p = reinterpret_cast<const uint4*>(d + k);
-      c0 = __ldg(p);
-      c1 = __ldg(p + 1);
+      if constexpr (SMEM) {
+        c0 = p[0];
+        c1 = p[1];
+      } else {
+        c0 = __ldg(p);
+        c1 = __ldg(p + 1);
+      }
     }
   }
 };
 
-template <int NSLOT, int E, class OUT>
-__device__ int expand_rlev2(InRing<NSLOT>& in, OUT& out, const RleDesc* __restrict__ d, uint32_t nd) {
+// Descriptors [k0, k1), whose first value is value n of the chunk; n is advanced.
+template <int NSLOT, int E, bool SMEM, class OUT>
+__device__ int expand_rlev2_range(InRing<NSLOT>& in, OUT& out, const RleDesc* __restrict__ d, uint32_t k0, uint32_t k1,
+                                  uint32_t& n) {
   constexpr uint64_t M = emask<E>();
   const uint32_t lane = in.lane;
   const uint32_t lo = in.lo;
-  uint32_t n = 0;
   int st = CODAG_OK;
   DescCache cur, nxt;
-  cur.load(d, 0, nd, lane);
-  nxt.load(d, 32, nd, lane);
-  for (uint32_t k = 0; k < nd; k++) {
-    const uint32_t src = k & 31u;
-    if (src == 0 && k) {
+  cur.template load<SMEM>(d, k0, k1, lane);
+  nxt.template load<SMEM>(d, k0 + 32, k1, lane);
+  for (uint32_t k = k0; k < k1; k++) {
+    const uint32_t src = (k - k0) & 31u;
+    if (src == 0 && k != k0) {
       cur = nxt;
-      nxt.load(d, k + 32, nd, lane);
+      nxt.template load<SMEM>(d, k + 32, k1, lane);
     }
     const uint32_t pos = lo + __shfl_sync(FULL, cur.c0.x, src);
     const uint32_t info = __shfl_sync(FULL, cur.c0.y, src);
@@ -261,26 +378,34 @@ __device__ int expand_rlev2(InRing<NSLOT>& in, OUT& out, const RleDesc* __restri
     __syncwarp();
     out.flush_to(n * E);
   }
+  return st;
+}
+
+template <int NSLOT, int E, class OUT>
+__device__ int expand_rlev2(InRing<NSLOT>& in, OUT& out, const RleDesc* __restrict__ d, uint32_t nd) {
+  uint32_t n = 0;
+  int st = expand_rlev2_range<NSLOT, E, false>(in, out, d, 0, nd, n);
   if (!in.drain() && st == CODAG_OK) st = CODAG_ETIMEOUT;
   out.finish(n * E);
   if (st == CODAG_OK && n * E < out.store) st = CODAG_ECORRUPT;
   return st;
 }
 
-template <int NSLOT, int E, class OUT>
-__device__ int expand_rlev1(InRing<NSLOT>& in, OUT& out, const RleDesc* __restrict__ d, uint32_t nd) {
+// Descriptors [k0, k1), whose first value is value n of the chunk; n is advanced.
+template <int NSLOT, int E, bool SMEM, class OUT>
+__device__ int expand_rlev1_range(InRing<NSLOT>& in, OUT& out, const RleDesc* __restrict__ d, uint32_t k0, uint32_t k1,
+                                  uint32_t& n) {
   const uint32_t lane = in.lane;
   const uint32_t lo = in.lo;
-  uint32_t n = 0;
   int st = CODAG_OK;
   DescCache cur, nxt;
-  cur.load(d, 0, nd, lane);
-  nxt.load(d, 32, nd, lane);
-  for (uint32_t k = 0; k < nd; k++) {
-    const uint32_t src = k & 31u;
-    if (src == 0 && k) {
+  cur.template load<SMEM>(d, k0, k1, lane);
+  nxt.template load<SMEM>(d, k0 + 32, k1, lane);
+  for (uint32_t k = k0; k < k1; k++) {
+    const uint32_t src = (k - k0) & 31u;
+    if (src == 0 && k != k0) {
       cur = nxt;
-      nxt.load(d, k + 32, nd, lane);
+      nxt.template load<SMEM>(d, k + 32, k1, lane);
     }
     const uint32_t pos = lo + __shfl_sync(FULL, cur.c0.x, src);
     const uint32_t info = __shfl_sync(FULL, cur.c0.y, src);
@@ -301,6 +426,13 @@ __device__ int expand_rlev1(InRing<NSLOT>& in, OUT& out, const RleDesc* __restri
     __syncwarp();
     out.flush_to(n * E);
   }
+  return st;
+}
+
+template <int NSLOT, int E, class OUT>
+__device__ int expand_rlev1(InRing<NSLOT>& in, OUT& out, const RleDesc* __restrict__ d, uint32_t nd) {
+  uint32_t n = 0;
+  int st = expand_rlev1_range<NSLOT, E, false>(in, out, d, 0, nd, n);
   if (!in.drain() && st == CODAG_OK) st = CODAG_ETIMEOUT;
   out.finish(n * E);
   if (st == CODAG_OK && n * E < out.store) st = CODAG_ECORRUPT;

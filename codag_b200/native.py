@@ -41,7 +41,8 @@ class HBuf(C.Structure):
 
 
 class Tune(C.Structure):
-    _fields_ = [("warps_per_cta", C.c_int32), ("ring_slots", C.c_int32), ("lut_bits", C.c_int32), ("reserved", C.c_int32)]
+    _fields_ = [("warps_per_cta", C.c_int32), ("ring_slots", C.c_int32), ("lut_bits", C.c_int32),
+                ("cta_per_chunk", C.c_int32)]
 
 
 class ChunkDesc(C.Structure):
@@ -206,8 +207,8 @@ def gen_text(nbytes: int, seed: int) -> np.ndarray:
 
 
 # --- tuning ---------------------------------------------------------------------------------
-def set_tune(codec: int, warps_per_cta: int, ring_slots: int, lut_bits: int = 10) -> None:
-    t = Tune(warps_per_cta, ring_slots, lut_bits, 0)
+def set_tune(codec: int, warps_per_cta: int, ring_slots: int, lut_bits: int = 10, cta_per_chunk: int = 0) -> None:
+    t = Tune(warps_per_cta, ring_slots, lut_bits, cta_per_chunk)
     check("codag_set_tune", lib().codag_set_tune(codec, C.byref(t)))
 
 

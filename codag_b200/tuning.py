@@ -4,6 +4,7 @@ Per codec it times every supported combination of
   warps_per_cta  chunks decoded by one CTA (one warp per chunk): 1, 2, 4, 8
   ring_slots     depth of the TMA input ring in 1 KiB slots: 4, 8 (2 also for Deflate)
   lut_bits       primary Huffman table width (Deflate only): 9, 10, 11
+  cta_per_chunk  RLE only: a whole CTA of 4 or 8 warps per chunk instead of one warp
 on a resident sample of the caller's chunks, keeps the fastest, installs it with
 codag_set_tune and caches it in a JSON file keyed by GPU name and codec, so later runs
 on the same kind of GPU skip the search.  Batched plans take their shape the same way
@@ -27,7 +28,8 @@ def candidates(codec: int):
     warps = (1, 2, 4, 8)
     if codec == native.DEFLATE:
         return list(itertools.product(warps, (2, 4, 8), (9, 10, 11)))
-    return list(itertools.product(warps, (4, 8), (10,)))
+    # one warp per chunk, or one CTA of 4 or 8 warps per chunk
+    return list(itertools.product(warps, (4, 8), (10,), (0,))) + [(4, 4, 10, 1), (8, 4, 10, 1)]
 
 
 def _key(codec: int, tag: str) -> str:
