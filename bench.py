@@ -318,7 +318,8 @@ def run_ours(args, rank: int, world: int, local: int):
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": KERNEL_NAMES[codec], "alg_bytes_per_launch": alg_bytes,
+                     "kernel": ("k_rle_cta<RLEV1/RLEV2, E>" if codec != 2 and nat.get_tune(codec).cta_per_chunk
+                                else KERNEL_NAMES[codec]), "alg_bytes_per_launch": alg_bytes,
                      "note": ("launch = header walk + expansion kernels of one call" if codec != 2 and args.rle_passes == 2
                               else "one kernel"),
                      "launch_ms": round(per_launch * 1e3, 4)},
