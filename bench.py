@@ -362,6 +362,9 @@ def main():
             if args.workload == "batched":
                 from codag_b200 import batched_bench
                 batched_bench.run_reference(args)
+            elif args.workload == "serving":
+                print(json.dumps({"impl": "reference", "unavailable": "the serving loop has no CPU counterpart; "
+                                  "the per-codec workloads time the CPU decoders"}), flush=True)
             else:
                 run_reference(args)
         return
