@@ -1,0 +1,91 @@
+"""Deflate chunks with adversarial back-references, written by Python's zlib with random
+levels, strategies, window sizes and memory levels: periodic data whose period straddles the
+decoder's 4 KiB shared-memory window (4095, 4096, 4097 bytes) or reaches the 32 KiB maximum
+distance, byte runs (distance-1, length-258 copies), short periods (overlapping copies),
+incompressible bytes (stored blocks) and mixtures of them.
+
+CPU: the oracle must decode every chunk to its source.  GPU: one launch over all chunks must
+match the source byte for byte, with every chunk's status OK."""
+import zlib
+
+import numpy as np
+import pytest
+
+CH = 131072
+PERIODS = [1, 2, 3, 5, 31, 255, 256, 257, 4095, 4096, 4097, 4098, 8191, 16384, 32767, 32768]
+
+
+def _chunk(rng: np.random.Generator, kind: int) -> np.ndarray:
+    if kind == 0:  # one period over the whole chunk
+        p = int(rng.choice(PERIODS))
+        return np.resize(rng.integers(0, 256, p, dtype=np.uint8), CH)
+    if kind == 1:  # incompressible
+        return rng.integers(0, 256, CH, dtype=np.uint8)
+    # segments of runs, periods and noise; periods repeat a block seen earlier in the chunk
+    out = np.empty(CH, np.uint8)
+    i = 0
+    while i < CH:
+        n = min(CH - i, int(rng.integers(1, 20000)))
+        t = int(rng.integers(0, 4))
+        if t == 0:
+            out[i:i + n] = rng.integers(0, 256, dtype=np.uint8)
+        elif t == 1:
+            out[i:i + n] = rng.integers(0, 256, n, dtype=np.uint8)
+        elif t == 2 and i >= 4097:
+            d = int(rng.choice([4095, 4096, 4097, min(i, 32768)]))
+            k = 0
+            while k < n:  # a copy at distance d (repeating itself when n > d)
+                m = min(d, n - k)
+                out[i + k:i + k + m] = out[i + k - d:i + k - d + m]
+                k += m
+        else:
+            p = int(rng.choice(PERIODS[:8]))
+            out[i:i + n] = np.resize(rng.integers(0, 256, p, dtype=np.uint8), n)
+        i += n
+    return out
+
+
+def _streams(seed: int, n: int):
+    """n chunks of CH bytes, zlib-wrapped, each padded to 8 bytes: (comp, rel offsets, source)."""
+    rng = np.random.default_rng(seed)
+    parts, rel, src = [], [0], []
+    for c in range(n):
+        data = _chunk(rng, c % 3)
+        level = int(rng.integers(0, 10))
+        strategy = int(rng.choice([0, 1, 2, 3, 4]))
+        wbits = int(rng.integers(9, 16))
+        mem = int(rng.integers(1, 10))
+        co = zlib.compressobj(level, zlib.DEFLATED, wbits, mem, strategy)
+        s = co.compress(data.tobytes()) + co.flush()
+        s += b"\0" * ((-len(s)) % 8)
+        parts.append(s)
+        rel.append(rel[-1] + len(s))
+        src.append(data)
+    return np.frombuffer(b"".join(parts), np.uint8).copy(), np.array(rel, np.uint64), np.concatenate(src)
+
+
+def test_oracle_decodes_adversarial_chunks(oracle):
+    comp, rel, src = _streams(1, 12)
+    for i in range(rel.size - 1):
+        st, out = oracle.deflate_chunk(comp[int(rel[i]):int(rel[i + 1])], CH)
+        assert st == 0, i
+        assert np.array_equal(out[:CH], src[i * CH:(i + 1) * CH]), i
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", [2, 3])
+def test_gpu_decodes_adversarial_chunks(cuda, native, seed):
+    from codag_b200 import api
+    comp, rel, src = _streams(seed, 36)
+    n = rel.size - 1
+    d_comp = cuda.from_numpy(comp).to("cuda")
+    d_rel = cuda.from_numpy(rel.view(np.int64)).to("cuda")
+    out = cuda.full((n * CH + 64,), 0xA5, dtype=cuda.uint8, device="cuda")
+    st = cuda.full((n,), -1, dtype=cuda.int32, device="cuda")
+    api.decompress_deflate(d_comp, d_rel, CH, out, 2, n * CH, st)
+    cuda.cuda.synchronize()
+    o = out.cpu().numpy()
+    assert st.cpu().numpy().tolist() == [0] * n
+    assert np.all(o[n * CH:] == 0xA5)
+    bad = np.flatnonzero(o[:n * CH] != src)
+    assert bad.size == 0, (int(bad[0]) // CH, int(bad[0]) % CH)
