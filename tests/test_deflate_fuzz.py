@@ -1,8 +1,8 @@
 """Deflate chunks with adversarial back-references, written by Python's zlib with random
 levels, strategies, window sizes and memory levels: periodic data whose period straddles the
-decoder's 4 KiB shared-memory window (4095, 4096, 4097 bytes) or reaches the 32 KiB maximum
-distance, byte runs (distance-1, length-258 copies), short periods (overlapping copies),
-incompressible bytes (stored blocks) and mixtures of them.
+decoder's shared-memory windows (2 KiB in the plain kernel, 4 KiB in the batch kernel) or
+reaches the 32 KiB maximum distance, byte runs (distance-1, length-258 copies), short periods
+(overlapping copies), incompressible bytes (stored blocks) and mixtures of them.
 
 CPU: the oracle must decode every chunk to its source.  GPU: one launch over all chunks must
 match the source byte for byte, with every chunk's status OK."""
@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 CH = 131072
-PERIODS = [1, 2, 3, 5, 31, 255, 256, 257, 4095, 4096, 4097, 4098, 8191, 16384, 32767, 32768]
+PERIODS = [1, 2, 3, 5, 31, 255, 256, 257, 2047, 2048, 2049, 4095, 4096, 4097, 8191, 16384, 32767, 32768]
 
 
 def _chunk(rng: np.random.Generator, kind: int) -> np.ndarray:
@@ -32,7 +32,7 @@ def _chunk(rng: np.random.Generator, kind: int) -> np.ndarray:
         elif t == 1:
             out[i:i + n] = rng.integers(0, 256, n, dtype=np.uint8)
         elif t == 2 and i >= 4097:
-            d = int(rng.choice([4095, 4096, 4097, min(i, 32768)]))
+            d = int(rng.choice([2047, 2048, 2049, 4095, 4096, 4097, min(i, 32768)]))
             k = 0
             while k < n:  # a copy at distance d (repeating itself when n > d)
                 m = min(d, n - k)
@@ -89,3 +89,26 @@ def test_gpu_decodes_adversarial_chunks(cuda, native, seed):
     assert np.all(o[n * CH:] == 0xA5)
     bad = np.flatnonzero(o[:n * CH] != src)
     assert bad.size == 0, (int(bad[0]) // CH, int(bad[0]) % CH)
+
+
+@pytest.mark.gpu
+def test_batch_kernel_decodes_adversarial_chunks(cuda, native):
+    """The same streams through the batched persistent launch (its 4 KiB window)."""
+    from codag_b200 import api
+    comp, rel, src = _streams(4, 24)
+    n = rel.size - 1
+    streams = [comp[int(rel[i]):int(rel[i + 1])] for i in range(n)]
+    cs = api.pack_chunks(streams, [native.DEFLATE] * n, [1] * n, [CH] * n)
+    plan = api.BatchPlan(cs.descs)
+    try:
+        out = cuda.zeros(cs.out_bytes, dtype=cuda.uint8, device="cuda")
+        st = cuda.full((n,), -1, dtype=cuda.int32, device="cuda")
+        plan.run(cuda.from_numpy(cs.comp).to("cuda"), out, st)
+        cuda.cuda.synchronize()
+    finally:
+        plan.close()
+    assert st.cpu().numpy().tolist() == [0] * n
+    o = out.cpu().numpy()
+    for i in range(n):
+        a = int(cs.descs[i]["out_off"])
+        assert np.array_equal(o[a:a + CH], src[i * CH:(i + 1) * CH]), i
