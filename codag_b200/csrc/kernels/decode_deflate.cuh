@@ -226,6 +226,11 @@ struct BitReader {
 template <int NSLOT, int LB, class OUT>
 __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<LB>& sc, uint64_t chunk_bytes,
                                     uint32_t wrapper) {
+  // Before each symbol fewer than kFlush bytes of the window are unflushed; what is written
+  // until the next flush (a match of up to 258 bytes, a piece of a stored block) must not wrap
+  // onto them.
+  static_assert(OUT::kBytes - OUT::kFlush >= 258, "window too small for a match");
+  constexpr uint32_t kStoredPiece = OUT::kBytes - OUT::kFlush < 1024u ? OUT::kBytes - OUT::kFlush : 1024u;
   const uint32_t lane = in.lane;
   const uint32_t cap = static_cast<uint32_t>(chunk_bytes);
   const HuffTable lit{sc.lit_lut, sc.lit_sorted, sc.lit_cnt, sc.lit_first, sc.lit_index, LB};
@@ -282,7 +287,7 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<
       if (p + len > in.hi || op + len > cap) { st = CODAG_ECORRUPT; break; }
       uint32_t left = len;
       while (left) {
-        const uint32_t piece = left < 1024u ? left : 1024u;
+        const uint32_t piece = left < kStoredPiece ? left : kStoredPiece;
         if (!in.release(p)) { st = CODAG_ETIMEOUT; break; }
         st = in.ensure(p + piece);
         if (st) break;

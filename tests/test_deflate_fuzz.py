@@ -1,6 +1,6 @@
 """Deflate chunks with adversarial back-references, written by Python's zlib with random
 levels, strategies, window sizes and memory levels: periodic data whose period straddles the
-decoder's shared-memory windows (2 KiB in the plain kernel, 4 KiB in the batch kernel) or
+decoder's shared-memory windows (1 KiB in the plain kernel, 4 KiB in the batch kernel) or
 reaches the 32 KiB maximum distance, byte runs (distance-1, length-258 copies), short periods
 (overlapping copies), incompressible bytes (stored blocks) and mixtures of them.
 
@@ -12,7 +12,8 @@ import numpy as np
 import pytest
 
 CH = 131072
-PERIODS = [1, 2, 3, 5, 31, 255, 256, 257, 2047, 2048, 2049, 4095, 4096, 4097, 8191, 16384, 32767, 32768]
+PERIODS = [1, 2, 3, 5, 31, 255, 256, 257, 1023, 1024, 1025, 2047, 2048, 2049, 4095, 4096, 4097, 8191, 16384,
+           32767, 32768]
 
 
 def _chunk(rng: np.random.Generator, kind: int) -> np.ndarray:
@@ -32,7 +33,7 @@ def _chunk(rng: np.random.Generator, kind: int) -> np.ndarray:
         elif t == 1:
             out[i:i + n] = rng.integers(0, 256, n, dtype=np.uint8)
         elif t == 2 and i >= 4097:
-            d = int(rng.choice([2047, 2048, 2049, 4095, 4096, 4097, min(i, 32768)]))
+            d = int(rng.choice([1023, 1024, 1025, 2047, 2048, 4095, 4096, 4097, min(i, 32768)]))
             k = 0
             while k < n:  # a copy at distance d (repeating itself when n > d)
                 m = min(d, n - k)
