@@ -29,13 +29,22 @@ constexpr uint32_t align_up(uint32_t v, uint32_t a) { return (v + a - 1) / a * a
 
 using RleOut = OutRing<12, 10, true>;  // 4 KiB ring, 1 KiB drains by TMA bulk stores
 using InflateOut = OutRing<12, 10>;  // 4 KiB window, 1 KiB drains (the batch kernel decodes RLE into it too)
-// The plain Deflate kernel's window: 1 KiB, 256 B drains.  The smaller window sends more
-// back-references to the flushed output in global memory (a copy whose source ends more than
-// 508 bytes back is always flushed already), but a warp then needs 7.5 KiB of shared memory
-// instead of 10.5 KiB, so 28 warps per SM are resident instead of 20: 1 GiB of text decodes
-// in 22.6 ms instead of 24.8 ms (4 KiB window).  The batch kernel keeps 4 KiB: an RLE header
-// can write 2,040 bytes at once.
-using InflateWin = OutRing<10, 8>;
+// The plain Deflate kernel sizes its window with the literal table (lut_bits), at two
+// measured points.  9 bits: 1 KiB window, 256 B drains, 7.5 KiB of shared memory per warp, 28
+// warps per SM; more back-references read the flushed output in global memory (a copy whose
+// source ends more than 508 bytes back is always flushed already) and more codes miss the
+// table, but with many chunks the extra resident warps win: 1 GiB of text in 22.6 ms.  10 or
+// 11 bits: 2 KiB window, 512 B drains (10.5 KiB per warp with 10 bits, 20 warps per SM): 25%
+// fewer instructions per chunk, faster when there are too few chunks to fill the SMs.  The
+// batch kernel keeps 4 KiB: an RLE header can write 2,040 bytes at once.
+template <int LB>
+struct InflateWinOf {
+  using T = OutRing<11, 9>;
+};
+template <>
+struct InflateWinOf<9> {
+  using T = OutRing<10, 8>;
+};
 
 template <int NSLOT>
 struct RleLayout {
@@ -153,7 +162,8 @@ __global__ void __launch_bounds__(256) k_inflate_plain(const uint8_t* __restrict
                                                        uint8_t* __restrict__ out, uint64_t out_bytes,
                                                        int32_t* __restrict__ status, uint64_t wait_cycles) {
   extern __shared__ __align__(128) uint8_t smem[];
-  using L = InflateLayout<NSLOT, LB, InflateWin>;
+  using W = typename InflateWinOf<LB>::T;
+  using L = InflateLayout<NSLOT, LB, W>;
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint64_t chunk = static_cast<uint64_t>(blockIdx.x) * (blockDim.x >> 5) + warp;
   if (chunk >= n_chunks) return;
@@ -165,7 +175,7 @@ __global__ void __launch_bounds__(256) k_inflate_plain(const uint8_t* __restrict
   in.phase = 0;
   in.wait_cycles = wait_cycles;
   in.lane = lane;
-  InflateWin o;
+  W o;
   o.buf = base + L::kOut;
   o.sbuf = smem_u32(o.buf);
   o.lane = lane;
@@ -502,7 +512,7 @@ template <int NSLOT, int LB>
 codag_status launch_inflate(const codag_tune& t, const uint8_t* comp, uint64_t comp_bytes, const uint64_t* blk_off,
                             uint64_t n, uint64_t chunk_bytes, int wrapper, uint8_t* out, uint64_t out_bytes,
                             int32_t* status, cudaStream_t s) {
-  using L = InflateLayout<NSLOT, LB, InflateWin>;
+  using L = InflateLayout<NSLOT, LB, typename InflateWinOf<LB>::T>;
   const uint32_t smem = L::kPerWarp * t.warps_per_cta;
   auto kern = k_inflate_plain<NSLOT, LB>;
   if (allow_smem(kern, smem) != cudaSuccess) return CODAG_ECUDA;

@@ -121,7 +121,9 @@ codag_status codag_decompress_deflate(const uint8_t *d_comp, uint64_t comp_bytes
  * the number of chunks one CTA decodes (one warp per chunk, 1..8); ring_slots the depth of
  * the TMA input ring (2, 4 or 8 slots of 1 KiB; the RLE codecs need at least 4 because an
  * RLE v2 header with its data spans up to 2060 bytes); lut_bits the primary Huffman table width
- * (Deflate only: 9, 10 or 11).  cta_per_chunk (RLE only, 0 or 1) switches the RLE calls
+ * (Deflate only: 9, 10 or 11), which also sizes the shared-memory history window of the
+ * Deflate call (9: 1 KiB, so more warps fit per SM, for many chunks; 10 and 11: 2 KiB, fewer
+ * instructions per chunk, for few chunks).  cta_per_chunk (RLE only, 0 or 1) switches the RLE calls
  * without a workspace to one CTA of warps_per_cta warps per chunk: the CTA stages the
  * chunk's stream in shared memory, one warp walks its headers and all warps expand them,
  * which shortens the decode of a single chunk (few chunks, e.g. an 8 MiB column) at the cost

@@ -74,8 +74,9 @@ def test_oracle_decodes_adversarial_chunks(oracle):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("lut", [9, 10, 11])  # 9 bits: 1 KiB window; 10 and 11: 2 KiB
 @pytest.mark.parametrize("seed", [2, 3])
-def test_gpu_decodes_adversarial_chunks(cuda, native, seed):
+def test_gpu_decodes_adversarial_chunks(cuda, native, seed, lut):
     from codag_b200 import api
     comp, rel, src = _streams(seed, 36)
     n = rel.size - 1
@@ -83,8 +84,13 @@ def test_gpu_decodes_adversarial_chunks(cuda, native, seed):
     d_rel = cuda.from_numpy(rel.view(np.int64)).to("cuda")
     out = cuda.full((n * CH + 64,), 0xA5, dtype=cuda.uint8, device="cuda")
     st = cuda.full((n,), -1, dtype=cuda.int32, device="cuda")
-    api.decompress_deflate(d_comp, d_rel, CH, out, 2, n * CH, st)
-    cuda.cuda.synchronize()
+    old = native.get_tune(native.DEFLATE)
+    native.set_tune(native.DEFLATE, old.warps_per_cta, old.ring_slots, lut)
+    try:
+        api.decompress_deflate(d_comp, d_rel, CH, out, 2, n * CH, st)
+        cuda.cuda.synchronize()
+    finally:
+        native.set_tune(native.DEFLATE, old.warps_per_cta, old.ring_slots, old.lut_bits)
     o = out.cpu().numpy()
     assert st.cpu().numpy().tolist() == [0] * n
     assert np.all(o[n * CH:] == 0xA5)
