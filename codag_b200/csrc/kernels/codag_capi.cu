@@ -79,6 +79,8 @@ __device__ __forceinline__ uint64_t store_bytes(uint64_t base, uint64_t chunk_by
   return base < out_bytes ? (chunk_bytes < out_bytes - base ? chunk_bytes : out_bytes - base) : 0;
 }
 
+__device__ __forceinline__ bool valid_elem_dev(uint32_t e) { return e == 1 || e == 2 || e == 4 || e == 8; }
+
 __device__ __forceinline__ bool stream_in_bounds(uint64_t off, uint64_t len, uint64_t comp_bytes) {
   return off <= comp_bytes && len <= comp_bytes - off && len < (1ull << 28);
 }
@@ -198,14 +200,19 @@ __global__ void __launch_bounds__(256) k_inflate_plain(const uint8_t* __restrict
 // ---------------------------------------------------------------------------------------
 // batched persistent kernel
 // ---------------------------------------------------------------------------------------
-template <int NSLOT, int LB>
+// SMALL: the Deflate window is the plain kernel's (InflateWinOf<LB>), for more resident warps;
+// then every RLE output must be element aligned (values go straight to global memory), which
+// the host checks before it picks this form.  Otherwise the window is 4 KiB and an unaligned
+// RLE output goes through it.
+template <int NSLOT, int LB, bool SMALL>
 __global__ void __launch_bounds__(256) k_batch(const codag_chunk_desc* __restrict__ descs,
                                                const uint32_t* __restrict__ order, uint64_t n,
                                                uint32_t* __restrict__ queue, const uint8_t* __restrict__ comp,
                                                uint64_t comp_bytes, uint8_t* __restrict__ out, uint64_t out_bytes,
                                                int32_t* __restrict__ status, uint64_t wait_cycles) {
   extern __shared__ __align__(128) uint8_t smem[];
-  using L = InflateLayout<NSLOT, LB>;
+  using W = std::conditional_t<SMALL, typename InflateWinOf<LB>::T, InflateOut>;
+  using L = InflateLayout<NSLOT, LB, W>;
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   uint8_t* base = smem + warp * L::kPerWarp;
   InRing<NSLOT> in;
@@ -215,10 +222,12 @@ __global__ void __launch_bounds__(256) k_batch(const codag_chunk_desc* __restric
   in.phase = 0;
   in.wait_cycles = wait_cycles;
   in.lane = lane;
-  InflateOut o;
+  W o;
   o.buf = base + L::kOut;
   o.sbuf = smem_u32(o.buf);
   o.lane = lane;
+  DirectOut od;
+  od.lane = lane;
   auto& sc = *reinterpret_cast<InflateScratch<LB>*>(base + L::kScratch);
   init_ring_barriers<NSLOT>(in.bar, lane);
 
@@ -235,12 +244,22 @@ __global__ void __launch_bounds__(256) k_batch(const codag_chunk_desc* __restric
       st = CODAG_ECORRUPT;
     } else {
       in.begin(comp + d.comp_off, d.comp_len);
-      o.begin(out + d.out_off, d.out_len);
-      switch (d.codec) {
-        case CODAG_CODEC_RLEV1:
-        case CODAG_CODEC_RLEV2: st = decode_rle_any<NSLOT>(d.codec, in, o, d.out_len, d.elem_bytes); break;
-        case CODAG_CODEC_DEFLATE: st = decode_deflate_chunk<NSLOT, LB>(in, o, sc, d.out_len, d.wrapper_bytes); break;
-        default: st = CODAG_EINVAL;
+      if (d.codec == CODAG_CODEC_DEFLATE) {
+        o.begin(out + d.out_off, d.out_len);
+        st = decode_deflate_chunk<NSLOT, LB>(in, o, sc, d.out_len, d.wrapper_bytes);
+      } else if (d.codec == CODAG_CODEC_RLEV1 || d.codec == CODAG_CODEC_RLEV2) {
+        const uint32_t e = d.elem_bytes;
+        if (valid_elem_dev(e) && (reinterpret_cast<uintptr_t>(out + d.out_off) % e) == 0 && d.out_len % e == 0) {
+          od.begin(out + d.out_off, d.out_len);
+          st = decode_rle_any<NSLOT>(d.codec, in, od, d.out_len, static_cast<int>(e));
+        } else if constexpr (!SMALL) {
+          o.begin(out + d.out_off, d.out_len);
+          st = decode_rle_any<NSLOT>(d.codec, in, o, d.out_len, d.elem_bytes);
+        } else {
+          st = CODAG_EINVAL;
+        }
+      } else {
+        st = CODAG_EINVAL;
       }
     }
     if (status && lane == 0) status[i] = st;
@@ -685,7 +704,9 @@ struct codag_plan {
   codag_chunk_desc* d_descs = nullptr;
   uint32_t* d_order = nullptr;
   uint32_t* d_queue = nullptr;
-  int grid = 0;
+  int grid = 0;        // CTAs of the 4 KiB-window form
+  bool small = false;  // every RLE output offset is element aligned: the small-window form may run
+  int grid_small = 0;  // CTAs of the small-window form
   // captured graph and the arguments it was captured with
   cudaGraphExec_t exec = nullptr;
   const void* g_comp = nullptr;
@@ -696,11 +717,14 @@ struct codag_plan {
 
 namespace {
 
-template <int NSLOT, int LB>
-codag_status batch_setup(codag_plan* p) {
-  using L = InflateLayout<NSLOT, LB>;
+template <int NSLOT, int LB, bool SMALL>
+using BatchLayout = InflateLayout<NSLOT, LB, std::conditional_t<SMALL, typename InflateWinOf<LB>::T, InflateOut>>;
+
+template <int NSLOT, int LB, bool SMALL>
+codag_status batch_setup1(codag_plan* p) {
+  using L = BatchLayout<NSLOT, LB, SMALL>;
   const uint32_t smem = L::kPerWarp * p->tune.warps_per_cta;
-  auto kern = k_batch<NSLOT, LB>;
+  auto kern = k_batch<NSLOT, LB, SMALL>;
   if (allow_smem(kern, smem) != cudaSuccess) return CODAG_ECUDA;
   int dev = 0, sms = 0, per_sm = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
@@ -709,30 +733,37 @@ codag_status batch_setup(codag_plan* p) {
     return CODAG_ECUDA;
   per_sm = std::max(per_sm, 1);
   const uint64_t need = (p->n + p->tune.warps_per_cta - 1) / p->tune.warps_per_cta;
-  p->grid = static_cast<int>(std::min<uint64_t>(need, static_cast<uint64_t>(sms) * per_sm));
+  (SMALL ? p->grid_small : p->grid) = static_cast<int>(std::min<uint64_t>(need, static_cast<uint64_t>(sms) * per_sm));
   return CODAG_OK;
 }
 
 template <int NSLOT, int LB>
-void batch_launch(codag_plan* p, const uint8_t* comp, uint64_t comp_bytes, uint8_t* out, uint64_t out_bytes,
-                  int32_t* status, cudaStream_t s) {
-  using L = InflateLayout<NSLOT, LB>;
-  const uint32_t smem = L::kPerWarp * p->tune.warps_per_cta;
-  k_batch<NSLOT, LB><<<p->grid, 32 * p->tune.warps_per_cta, smem, s>>>(p->d_descs, p->d_order, p->n, p->d_queue, comp,
-                                                                       comp_bytes, out, out_bytes, status, wait_of());
+codag_status batch_setup(codag_plan* p) {
+  codag_status st = batch_setup1<NSLOT, LB, false>(p);
+  if (st == CODAG_OK && p->small) st = batch_setup1<NSLOT, LB, true>(p);
+  return st;
 }
 
-#define CODAG_BATCH_SWITCH(FN, ...)                      \
+template <int NSLOT, int LB, bool SMALL>
+void batch_launch(codag_plan* p, const uint8_t* comp, uint64_t comp_bytes, uint8_t* out, uint64_t out_bytes,
+                  int32_t* status, cudaStream_t s) {
+  using L = BatchLayout<NSLOT, LB, SMALL>;
+  const uint32_t smem = L::kPerWarp * p->tune.warps_per_cta;
+  k_batch<NSLOT, LB, SMALL><<<SMALL ? p->grid_small : p->grid, 32 * p->tune.warps_per_cta, smem, s>>>(
+      p->d_descs, p->d_order, p->n, p->d_queue, comp, comp_bytes, out, out_bytes, status, wait_of());
+}
+
+#define CODAG_BATCH_SWITCH(FN, SM, ...)                  \
   switch (p->tune.ring_slots * 100 + p->tune.lut_bits) { \
-    case 209: FN<2, 9>(__VA_ARGS__); break;              \
-    case 210: FN<2, 10>(__VA_ARGS__); break;             \
-    case 211: FN<2, 11>(__VA_ARGS__); break;             \
-    case 409: FN<4, 9>(__VA_ARGS__); break;              \
-    case 410: FN<4, 10>(__VA_ARGS__); break;             \
-    case 411: FN<4, 11>(__VA_ARGS__); break;             \
-    case 809: FN<8, 9>(__VA_ARGS__); break;              \
-    case 810: FN<8, 10>(__VA_ARGS__); break;             \
-    default: FN<8, 11>(__VA_ARGS__); break;              \
+    case 209: FN<2, 9, SM>(__VA_ARGS__); break;          \
+    case 210: FN<2, 10, SM>(__VA_ARGS__); break;         \
+    case 211: FN<2, 11, SM>(__VA_ARGS__); break;         \
+    case 409: FN<4, 9, SM>(__VA_ARGS__); break;          \
+    case 410: FN<4, 10, SM>(__VA_ARGS__); break;         \
+    case 411: FN<4, 11, SM>(__VA_ARGS__); break;         \
+    case 809: FN<8, 9, SM>(__VA_ARGS__); break;          \
+    case 810: FN<8, 10, SM>(__VA_ARGS__); break;         \
+    default: FN<8, 11, SM>(__VA_ARGS__); break;          \
   }
 
 codag_status batch_setup_any(codag_plan* p) {
@@ -755,7 +786,13 @@ codag_status batch_setup_any(codag_plan* p) {
 void batch_enqueue(codag_plan* p, const uint8_t* comp, uint64_t comp_bytes, uint8_t* out, uint64_t out_bytes,
                    int32_t* status, cudaStream_t s) {
   cudaMemsetAsync(p->d_queue, 0, sizeof(uint32_t), s);
-  CODAG_BATCH_SWITCH(batch_launch, p, comp, comp_bytes, out, out_bytes, status, s);
+  // the small-window form needs every RLE output element aligned: offsets (checked at plan
+  // time) and the base (8-byte aligned covers every element width)
+  if (p->small && (reinterpret_cast<uintptr_t>(out) & 7u) == 0) {
+    CODAG_BATCH_SWITCH(batch_launch, true, p, comp, comp_bytes, out, out_bytes, status, s);
+  } else {
+    CODAG_BATCH_SWITCH(batch_launch, false, p, comp, comp_bytes, out, out_bytes, status, s);
+  }
 }
 
 // work estimate used to order the queue: compressed bytes, Deflate weighted by its
@@ -781,6 +818,9 @@ extern "C" codag_status codag_batch_plan(const codag_chunk_desc* h_descs, uint64
   if (!p) return CODAG_ENOMEM;
   p->n = n;
   p->tune = t;
+  p->small = true;
+  for (uint64_t i = 0; i < n; i++)
+    if (h_descs[i].codec != CODAG_CODEC_DEFLATE && h_descs[i].out_off % h_descs[i].elem_bytes) p->small = false;
   std::vector<uint32_t> order(n);
   for (uint64_t i = 0; i < n; i++) order[i] = static_cast<uint32_t>(i);
   std::stable_sort(order.begin(), order.end(),

@@ -57,6 +57,38 @@ def test_batched_matches_source(cuda, small_set, shape, use_graph):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("how", ["base", "offsets"])
+def test_batched_unaligned_outputs(cuda, small_set, how):
+    """Outputs that are not element aligned route RLE values through the 4 KiB window of the
+    batch kernel: an output base off 8-byte alignment (the plan is aligned, the call is not), or
+    RLE output offsets shifted by one byte (the plan itself needs the 4 KiB form)."""
+    from codag_b200 import api
+    ms = small_set
+    descs = ms.descs.copy()
+    shift = 0
+    if how == "offsets":
+        descs["out_off"] = descs["out_off"] + 1
+    else:
+        shift = 3
+    d_comp = cuda.from_numpy(ms.comp).to("cuda")
+    buf = cuda.full((ms.out_bytes + 16,), 0x77, dtype=cuda.uint8, device="cuda")
+    d_out = buf[shift:]
+    st = cuda.full((ms.n,), -1, dtype=cuda.int32, device="cuda")
+    plan = api.BatchPlan(descs)
+    try:
+        plan.run(d_comp, d_out, st, use_graph=False)
+        cuda.cuda.synchronize()
+    finally:
+        plan.close()
+    assert not st.cpu().numpy().any()
+    got = d_out.cpu().numpy()
+    want = ms.expected()
+    for d0, d1, ln in zip(ms.descs, descs, ms.in_len):
+        o0, o1 = int(d0["out_off"]), int(d1["out_off"])
+        assert np.array_equal(got[o1:o1 + int(ln)], want[o0:o0 + int(ln)])
+
+
+@pytest.mark.gpu
 def test_per_file_path_matches_source(cuda, small_set):
     ms = small_set
     d_comp = cuda.from_numpy(ms.comp).to("cuda")
