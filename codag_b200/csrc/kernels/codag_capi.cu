@@ -28,7 +28,6 @@ namespace {
 constexpr uint32_t align_up(uint32_t v, uint32_t a) { return (v + a - 1) / a * a; }
 
 using RleOut = OutRing<12, 10, true>;  // 4 KiB ring, 1 KiB drains by TMA bulk stores
-using InflateOut = OutRing<12, 10>;  // 4 KiB window, 1 KiB drains (the batch kernel decodes RLE into it too)
 // The plain Deflate kernel sizes its window with the literal table (lut_bits), at two
 // measured points.  9 bits: 1 KiB window, 256 B drains, 7.5 KiB of shared memory per warp, 28
 // warps per SM; more back-references read the flushed output in global memory (a copy whose
@@ -36,7 +35,7 @@ using InflateOut = OutRing<12, 10>;  // 4 KiB window, 1 KiB drains (the batch ke
 // table, but with many chunks the extra resident warps win: 1 GiB of text in 22.6 ms.  10 or
 // 11 bits: 2 KiB window, 512 B drains (10.5 KiB per warp with 10 bits, 20 warps per SM): 25%
 // fewer instructions per chunk, faster when there are too few chunks to fill the SMs.  The
-// batch kernel keeps 4 KiB: an RLE header can write 2,040 bytes at once.
+// batch kernel uses the same windows: its RLE values never pass through them.
 template <int LB>
 struct InflateWinOf {
   using T = OutRing<11, 9>;
@@ -62,7 +61,7 @@ struct RleDirectLayout {
   static constexpr uint32_t kPerWarp = align_up(kBar + NSLOT * 8, 128);
 };
 
-template <int NSLOT, int LB, class OUT = InflateOut>
+template <int NSLOT, int LB, class OUT>
 struct InflateLayout {
   static constexpr uint32_t kIn = 0;
   static constexpr uint32_t kOut = kIn + NSLOT * kSlotBytes;
@@ -200,18 +199,17 @@ __global__ void __launch_bounds__(256) k_inflate_plain(const uint8_t* __restrict
 // ---------------------------------------------------------------------------------------
 // batched persistent kernel
 // ---------------------------------------------------------------------------------------
-// SMALL: the Deflate window is the plain kernel's (InflateWinOf<LB>), for more resident warps;
-// then every RLE output must be element aligned (values go straight to global memory), which
-// the host checks before it picks this form.  Otherwise the window is 4 KiB and an unaligned
-// RLE output goes through it.
-template <int NSLOT, int LB, bool SMALL>
+// The Deflate window is the plain kernel's (InflateWinOf<LB>), small enough for many resident
+// warps; RLE values go straight to global memory (element by element when the output is
+// element aligned, byte by byte otherwise), so no RLE header needs the window.
+template <int NSLOT, int LB>
 __global__ void __launch_bounds__(256) k_batch(const codag_chunk_desc* __restrict__ descs,
                                                const uint32_t* __restrict__ order, uint64_t n,
                                                uint32_t* __restrict__ queue, const uint8_t* __restrict__ comp,
                                                uint64_t comp_bytes, uint8_t* __restrict__ out, uint64_t out_bytes,
                                                int32_t* __restrict__ status, uint64_t wait_cycles) {
   extern __shared__ __align__(128) uint8_t smem[];
-  using W = std::conditional_t<SMALL, typename InflateWinOf<LB>::T, InflateOut>;
+  using W = typename InflateWinOf<LB>::T;
   using L = InflateLayout<NSLOT, LB, W>;
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   uint8_t* base = smem + warp * L::kPerWarp;
@@ -228,6 +226,8 @@ __global__ void __launch_bounds__(256) k_batch(const codag_chunk_desc* __restric
   o.lane = lane;
   DirectOut od;
   od.lane = lane;
+  ByteOut ob;
+  ob.lane = lane;
   auto& sc = *reinterpret_cast<InflateScratch<LB>*>(base + L::kScratch);
   init_ring_barriers<NSLOT>(in.bar, lane);
 
@@ -252,11 +252,9 @@ __global__ void __launch_bounds__(256) k_batch(const codag_chunk_desc* __restric
         if (valid_elem_dev(e) && (reinterpret_cast<uintptr_t>(out + d.out_off) % e) == 0 && d.out_len % e == 0) {
           od.begin(out + d.out_off, d.out_len);
           st = decode_rle_any<NSLOT>(d.codec, in, od, d.out_len, static_cast<int>(e));
-        } else if constexpr (!SMALL) {
-          o.begin(out + d.out_off, d.out_len);
-          st = decode_rle_any<NSLOT>(d.codec, in, o, d.out_len, d.elem_bytes);
         } else {
-          st = CODAG_EINVAL;
+          ob.begin(out + d.out_off, d.out_len);
+          st = decode_rle_any<NSLOT>(d.codec, in, ob, d.out_len, d.elem_bytes);
         }
       } else {
         st = CODAG_EINVAL;
@@ -704,9 +702,7 @@ struct codag_plan {
   codag_chunk_desc* d_descs = nullptr;
   uint32_t* d_order = nullptr;
   uint32_t* d_queue = nullptr;
-  int grid = 0;        // CTAs of the 4 KiB-window form
-  bool small = false;  // every RLE output offset is element aligned: the small-window form may run
-  int grid_small = 0;  // CTAs of the small-window form
+  int grid = 0;
   // captured graph and the arguments it was captured with
   cudaGraphExec_t exec = nullptr;
   const void* g_comp = nullptr;
@@ -717,14 +713,14 @@ struct codag_plan {
 
 namespace {
 
-template <int NSLOT, int LB, bool SMALL>
-using BatchLayout = InflateLayout<NSLOT, LB, std::conditional_t<SMALL, typename InflateWinOf<LB>::T, InflateOut>>;
+template <int NSLOT, int LB>
+using BatchLayout = InflateLayout<NSLOT, LB, typename InflateWinOf<LB>::T>;
 
-template <int NSLOT, int LB, bool SMALL>
-codag_status batch_setup1(codag_plan* p) {
-  using L = BatchLayout<NSLOT, LB, SMALL>;
+template <int NSLOT, int LB>
+codag_status batch_setup(codag_plan* p) {
+  using L = BatchLayout<NSLOT, LB>;
   const uint32_t smem = L::kPerWarp * p->tune.warps_per_cta;
-  auto kern = k_batch<NSLOT, LB, SMALL>;
+  auto kern = k_batch<NSLOT, LB>;
   if (allow_smem(kern, smem) != cudaSuccess) return CODAG_ECUDA;
   int dev = 0, sms = 0, per_sm = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
@@ -733,37 +729,30 @@ codag_status batch_setup1(codag_plan* p) {
     return CODAG_ECUDA;
   per_sm = std::max(per_sm, 1);
   const uint64_t need = (p->n + p->tune.warps_per_cta - 1) / p->tune.warps_per_cta;
-  (SMALL ? p->grid_small : p->grid) = static_cast<int>(std::min<uint64_t>(need, static_cast<uint64_t>(sms) * per_sm));
+  p->grid = static_cast<int>(std::min<uint64_t>(need, static_cast<uint64_t>(sms) * per_sm));
   return CODAG_OK;
 }
 
 template <int NSLOT, int LB>
-codag_status batch_setup(codag_plan* p) {
-  codag_status st = batch_setup1<NSLOT, LB, false>(p);
-  if (st == CODAG_OK && p->small) st = batch_setup1<NSLOT, LB, true>(p);
-  return st;
-}
-
-template <int NSLOT, int LB, bool SMALL>
 void batch_launch(codag_plan* p, const uint8_t* comp, uint64_t comp_bytes, uint8_t* out, uint64_t out_bytes,
                   int32_t* status, cudaStream_t s) {
-  using L = BatchLayout<NSLOT, LB, SMALL>;
+  using L = BatchLayout<NSLOT, LB>;
   const uint32_t smem = L::kPerWarp * p->tune.warps_per_cta;
-  k_batch<NSLOT, LB, SMALL><<<SMALL ? p->grid_small : p->grid, 32 * p->tune.warps_per_cta, smem, s>>>(
+  k_batch<NSLOT, LB><<<p->grid, 32 * p->tune.warps_per_cta, smem, s>>>(
       p->d_descs, p->d_order, p->n, p->d_queue, comp, comp_bytes, out, out_bytes, status, wait_of());
 }
 
-#define CODAG_BATCH_SWITCH(FN, SM, ...)                  \
+#define CODAG_BATCH_SWITCH(FN, ...)                      \
   switch (p->tune.ring_slots * 100 + p->tune.lut_bits) { \
-    case 209: FN<2, 9, SM>(__VA_ARGS__); break;          \
-    case 210: FN<2, 10, SM>(__VA_ARGS__); break;         \
-    case 211: FN<2, 11, SM>(__VA_ARGS__); break;         \
-    case 409: FN<4, 9, SM>(__VA_ARGS__); break;          \
-    case 410: FN<4, 10, SM>(__VA_ARGS__); break;         \
-    case 411: FN<4, 11, SM>(__VA_ARGS__); break;         \
-    case 809: FN<8, 9, SM>(__VA_ARGS__); break;          \
-    case 810: FN<8, 10, SM>(__VA_ARGS__); break;         \
-    default: FN<8, 11, SM>(__VA_ARGS__); break;          \
+    case 209: FN<2, 9>(__VA_ARGS__); break;              \
+    case 210: FN<2, 10>(__VA_ARGS__); break;             \
+    case 211: FN<2, 11>(__VA_ARGS__); break;             \
+    case 409: FN<4, 9>(__VA_ARGS__); break;              \
+    case 410: FN<4, 10>(__VA_ARGS__); break;             \
+    case 411: FN<4, 11>(__VA_ARGS__); break;             \
+    case 809: FN<8, 9>(__VA_ARGS__); break;              \
+    case 810: FN<8, 10>(__VA_ARGS__); break;             \
+    default: FN<8, 11>(__VA_ARGS__); break;              \
   }
 
 codag_status batch_setup_any(codag_plan* p) {
@@ -786,13 +775,7 @@ codag_status batch_setup_any(codag_plan* p) {
 void batch_enqueue(codag_plan* p, const uint8_t* comp, uint64_t comp_bytes, uint8_t* out, uint64_t out_bytes,
                    int32_t* status, cudaStream_t s) {
   cudaMemsetAsync(p->d_queue, 0, sizeof(uint32_t), s);
-  // the small-window form needs every RLE output element aligned: offsets (checked at plan
-  // time) and the base (8-byte aligned covers every element width)
-  if (p->small && (reinterpret_cast<uintptr_t>(out) & 7u) == 0) {
-    CODAG_BATCH_SWITCH(batch_launch, true, p, comp, comp_bytes, out, out_bytes, status, s);
-  } else {
-    CODAG_BATCH_SWITCH(batch_launch, false, p, comp, comp_bytes, out, out_bytes, status, s);
-  }
+  CODAG_BATCH_SWITCH(batch_launch, p, comp, comp_bytes, out, out_bytes, status, s);
 }
 
 // work estimate used to order the queue: compressed bytes, Deflate weighted by its
@@ -818,9 +801,6 @@ extern "C" codag_status codag_batch_plan(const codag_chunk_desc* h_descs, uint64
   if (!p) return CODAG_ENOMEM;
   p->n = n;
   p->tune = t;
-  p->small = true;
-  for (uint64_t i = 0; i < n; i++)
-    if (h_descs[i].codec != CODAG_CODEC_DEFLATE && h_descs[i].out_off % h_descs[i].elem_bytes) p->small = false;
   std::vector<uint32_t> order(n);
   for (uint64_t i = 0; i < n; i++) order[i] = static_cast<uint32_t>(i);
   std::stable_sort(order.begin(), order.end(),

@@ -10,10 +10,11 @@
 //   - keeps a 64-bit bit buffer refilled 32 bits at a time from the TMA input ring;
 //   - decodes a length or distance code together with its extra bits (one table entry
 //     gives both widths) and two literals per step where the table slot holds both codes;
-//   - expands back-references warp-cooperatively out of a 4 KiB shared-memory window of
-//     the output; older sources are read back from the chunk's already-written output,
-//     and such a load (length <= 32) is left in flight while the next symbols decode;
-//   - drains output in 1 KiB pieces with 16-byte vector stores;
+//   - expands back-references warp-cooperatively out of a shared-memory window of the
+//     output (the OUT ring: 1 or 2 KiB in the kernels here); older sources are read back
+//     from the chunk's already-written output, and such a load (length <= 32) is left in
+//     flight while the next symbols decode;
+//   - drains output in quarter-window pieces with vector stores;
 //   - decodes stored blocks.
 // Every lane runs the same symbol loop on the same data (shared-memory reads broadcast), so
 // control flow stays uniform and only the stores are lane-specific.

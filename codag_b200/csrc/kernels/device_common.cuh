@@ -506,4 +506,37 @@ struct DirectOut {
   }
 };
 
+// Output that is not element aligned, stored straight to global memory byte by byte (a
+// fallback for rare unaligned outputs that have no shared-memory ring to go through).
+struct ByteOut {
+  static constexpr uint32_t kFlush = 0xffffffffu;
+  static constexpr bool kDirect = false;
+  uint8_t* gdst;
+  uint32_t store;
+  uint32_t flushed;
+  uint32_t lane;
+
+  __device__ __forceinline__ void begin(uint8_t* dst, uint64_t store_bytes) {
+    gdst = dst;
+    store = static_cast<uint32_t>(store_bytes);
+    flushed = 0;
+  }
+  __device__ __forceinline__ void flush_to(uint32_t) {}
+  __device__ __forceinline__ void finish(uint32_t pos) { flushed = pos; }
+  template <int E>
+  __device__ __forceinline__ void put(uint32_t off, uint64_t v) {
+#pragma unroll
+    for (int i = 0; i < E; i++)
+      if (off + i < store) gdst[off + i] = static_cast<uint8_t>(v >> (8 * i));
+  }
+  template <int E>
+  __device__ __forceinline__ uint64_t get(uint32_t off) const {
+    uint64_t v = 0;
+#pragma unroll
+    for (int i = 0; i < E; i++)
+      if (off + i < store) v |= static_cast<uint64_t>(gdst[off + i]) << (8 * i);
+    return v;
+  }
+};
+
 }  // namespace codag_dev

@@ -59,9 +59,9 @@ def test_batched_matches_source(cuda, small_set, shape, use_graph):
 @pytest.mark.gpu
 @pytest.mark.parametrize("how", ["base", "offsets"])
 def test_batched_unaligned_outputs(cuda, small_set, how):
-    """Outputs that are not element aligned route RLE values through the 4 KiB window of the
-    batch kernel: an output base off 8-byte alignment (the plan is aligned, the call is not), or
-    RLE output offsets shifted by one byte (the plan itself needs the 4 KiB form)."""
+    """Outputs that are not element aligned: the batch kernel stores their RLE values byte by
+    byte.  Either the output base is off 8-byte alignment, or every output offset is shifted by
+    one byte."""
     from codag_b200 import api
     ms = small_set
     descs = ms.descs.copy()
