@@ -1,6 +1,6 @@
 """Deflate chunks with adversarial back-references, written by Python's zlib with random
 levels, strategies, window sizes and memory levels: periodic data whose period straddles the
-decoder's shared-memory windows (1 KiB in the plain kernel, 4 KiB in the batch kernel) or
+decoder's shared-memory windows (1 KiB with a 9-bit literal table, 2 KiB with 10 or 11 bits) or
 reaches the 32 KiB maximum distance, byte runs (distance-1, length-258 copies), short periods
 (overlapping copies), incompressible bytes (stored blocks) and mixtures of them.
 
@@ -100,7 +100,7 @@ def test_gpu_decodes_adversarial_chunks(cuda, native, seed, lut):
 
 @pytest.mark.gpu
 def test_batch_kernel_decodes_adversarial_chunks(cuda, native):
-    """The same streams through the batched persistent launch (its 4 KiB window)."""
+    """The same streams through the batched persistent launch."""
     from codag_b200 import api
     comp, rel, src = _streams(4, 24)
     n = rel.size - 1
