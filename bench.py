@@ -360,8 +360,8 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             if args.workload == "batched":
-                from codag_b200 import batched_bench
-                batched_bench.run_reference(args)
+                import bench_batched
+                bench_batched.run_reference(args)
             elif args.workload == "serving":
                 print(json.dumps({"impl": "reference", "unavailable": "the serving loop has no CPU counterpart; "
                                   "the per-codec workloads time the CPU decoders"}), flush=True)
@@ -375,11 +375,11 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     try:
         if args.workload == "batched":
-            from codag_b200 import batched_bench
-            batched_bench.main(args, rank, world, local)
+            import bench_batched
+            bench_batched.main(args, rank, world, local)
         elif args.workload == "serving":
-            from codag_b200 import serving_bench
-            serving_bench.main(args, rank, world, local)
+            import bench_serving
+            bench_serving.main(args, rank, world, local)
         else:
             run_ours(args, rank, world, local)
     finally:

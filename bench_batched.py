@@ -1,4 +1,4 @@
-"""`bench.py --workload batched`: CODAG's batched configuration on one GPU per rank.
+"""`bench.py --workload batched` (driver module beside bench.py): CODAG's batched configuration on one GPU per rank.
 
 Workload: 20,000 independently compressed files, decompressed size log-uniform 4 KiB-1 MiB
 (multiple of 8), 40% Deflate (Zipf text, zlib level 6), 30% RLE v1, 30% RLE v2, RLE values

@@ -1,4 +1,4 @@
-"""`bench.py --workload serving`: CODAG's serving configuration on one GPU.
+"""`bench.py --workload serving` (driver module beside bench.py): CODAG's serving configuration on one GPU.
 
 A pool of request files (log-uniform 64 KiB-256 MiB, 40/30/30 Deflate/RLE v1/RLE v2, CODAG's
 128 KiB chunk layout) is made resident in HBM; requests drawn uniformly from the pool arrive

@@ -12,7 +12,7 @@
 #include <string>
 #include <vector>
 
-#include "codag.h"
+#include "codag_format.h"
 
 namespace codag_cli {
 

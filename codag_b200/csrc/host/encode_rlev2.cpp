@@ -19,6 +19,7 @@
 #include <cstring>
 #include <vector>
 
+#include "../rlev2_widths.h"
 #include "host_common.hpp"
 
 namespace codag_host {
@@ -28,22 +29,6 @@ constexpr int kMaxLiterals = 128;  // utils.h:64
 constexpr int kMinRepeat = 3;      // utils.h:65
 constexpr int kMaxShortRepeat = 10;
 
-const uint8_t kWidthDecode[32] = {1,  2,  3,  4,  5,  6,  7,  8,  9,  10, 11, 12, 13, 14, 15, 16,
-                                  17, 18, 19, 20, 21, 22, 23, 24, 26, 28, 30, 32, 40, 48, 56, 64};
-const uint8_t kWidthEncode[65] = {0,  0,  1,  2,  3,  4,  5,  6,  7,  8,  9,  10, 11,
-                                  12, 13, 14, 15, 16, 17, 18, 19, 20, 21, 22, 23, 24,
-                                  24, 25, 25, 26, 26, 27, 27, 28, 28, 28, 28, 28, 28,
-                                  28, 28, 29, 29, 29, 29, 29, 29, 29, 29, 30, 30, 30,
-                                  30, 30, 30, 30, 30, 31, 31, 31, 31, 31, 31, 31, 31};
-const uint8_t kClosest[65] = {1,  1,  2,  3,  4,  5,  6,  7,  8,  9,  10, 11, 12, 13, 14, 15, 16,
-                              17, 18, 19, 20, 21, 22, 23, 24, 26, 26, 28, 28, 30, 30, 32, 32, 40,
-                              40, 40, 40, 40, 40, 40, 40, 48, 48, 48, 48, 48, 48, 48, 48, 56, 56,
-                              56, 56, 56, 56, 56, 56, 64, 64, 64, 64, 64, 64, 64, 64};
-const uint8_t kClosestAligned[65] = {
-    1,  1,  2,  4,  4,  8,  8,  8,  8,  16, 16, 16, 16, 16, 16, 16, 16, 24, 24, 24, 24, 24,
-    24, 24, 24, 32, 32, 32, 32, 32, 32, 32, 32, 40, 40, 40, 40, 40, 40, 40, 40, 48, 48, 48,
-    48, 48, 48, 48, 48, 56, 56, 56, 56, 56, 56, 56, 56, 64, 64, 64, 64, 64, 64, 64, 64};
-
 // number of significant bits rounded up to a representable width (find_closes_num_bits)
 inline uint8_t closest_width(uint64_t v) {
   uint8_t c = 0;
@@ -51,7 +36,7 @@ inline uint8_t closest_width(uint64_t v) {
     v >>= 1;
     ++c;
   }
-  return kClosest[c];
+  return v2_closest(c);
 }
 
 class RleV2Writer {
@@ -148,7 +133,7 @@ class RleV2Writer {
   // histogram of representable widths (compute_bit_width)
   static void width_hist(const uint64_t* d, uint32_t n, uint8_t* hist) {
     std::fill(hist, hist + 32, 0);
-    for (uint32_t i = 0; i < n; ++i) hist[kWidthEncode[closest_width(d[i])]]++;
+    for (uint32_t i = 0; i < n; ++i) hist[v2_code(closest_width(d[i]))]++;
   }
 
   // smallest width covering all but the top (100-p)% of values (compute_percentile_bit_width)
@@ -157,7 +142,7 @@ class RleV2Writer {
     int32_t left = (p == 0 ? 0 : static_cast<int32_t>((n * p - 1) / 100 + 1));
     for (int8_t i = 31; i >= 0; --i) {
       left -= hist[i];
-      if (left < 0) return kWidthDecode[i];
+      if (left < 0) return v2_width(i);
     }
     return 0;
   }
@@ -242,8 +227,8 @@ class RleV2Writer {
   void write_direct() {
     uint8_t hist[32];
     width_hist(lit_, nlit_, hist);
-    const uint8_t bits = kClosestAligned[percentile_width(hist, nlit_, 100)];
-    const uint16_t enc = kWidthEncode[bits];
+    const uint8_t bits = v2_closest_aligned(percentile_width(hist, nlit_, 100));
+    const uint16_t enc = v2_code(bits);
     // The reference writes var_runlen-1 here.  On every path var_runlen equals the number
     // of pending values except one: a 128-value run of zeros reaches this writer through
     // is_safe_subtract with var_runlen == 0, and the reference emits a length field of 511
@@ -260,7 +245,7 @@ class RleV2Writer {
   void write_delta() {
     uint16_t len;
     uint8_t enc = 0;
-    uint8_t bits = kClosestAligned[delta_bits_];
+    uint8_t bits = v2_closest_aligned(delta_bits_);
     if (fixed_delta_) {
       if (fix_ > kMinRepeat) {
         len = static_cast<uint16_t>(fix_ - 1);
@@ -271,7 +256,7 @@ class RleV2Writer {
       }
     } else {
       if (bits == 1) bits = 2;
-      enc = kWidthEncode[bits];
+      enc = v2_code(bits);
       len = static_cast<uint16_t>(var_ - 1);
       var_ = 0;
     }
@@ -288,7 +273,7 @@ class RleV2Writer {
   void write_patched(uint64_t lit_min, uint8_t b95, uint8_t b100, uint64_t* reduced) {
     // patch list (preparePatchedBlob1, encoder.h:182-268)
     int64_t mask = static_cast<int64_t>((static_cast<uint64_t>(1) << b95) - 1);
-    uint32_t pwidth = kClosest[b100 - b95];
+    uint32_t pwidth = v2_closest(b100 - b95);
     if (pwidth == 64) {
       pwidth = 56;
       b95 = 8;
@@ -332,19 +317,19 @@ class RleV2Writer {
 
     // header and body (writePatchedBasedValues, encoder.h:527-591)
     uint32_t len = var_ - 1;
-    const uint8_t h0 = static_cast<uint8_t>(0x80 | (kWidthEncode[b95] << 1) | ((len & 0x100) >> 8));
+    const uint8_t h0 = static_cast<uint8_t>(0x80 | (v2_code(b95) << 1) | ((len & 0x100) >> 8));
     const uint8_t h1 = static_cast<uint8_t>(len & 0xff);
     const uint32_t base_bits = closest_width(lit_min) + 1;
     const uint32_t base_bytes = (base_bits - 1) / 8 + 1;
-    const uint8_t h2 = static_cast<uint8_t>(((base_bytes - 1) << 5) | kWidthEncode[pwidth]);
+    const uint8_t h2 = static_cast<uint8_t>(((base_bytes - 1) << 5) | v2_code(pwidth));
     const uint8_t h3 = static_cast<uint8_t>((gap_width - 1) << 5 | nlist);
     put(h0);
     put(h1);
     put(h2);
     put(h3);
     for (int i = static_cast<int>(base_bytes) - 1; i >= 0; i--) put(static_cast<uint8_t>((lit_min >> (i * 8)) & 0xff));
-    put_unaligned(reduced, nlit_, kClosest[b95]);
-    put_unaligned(list, nlist, kClosest[gap_width + pwidth]);
+    put_unaligned(reduced, nlit_, v2_closest(b95));
+    put_unaligned(list, nlist, v2_closest(gap_width + pwidth));
     var_ = 0;
     nlit_ = 0;
   }

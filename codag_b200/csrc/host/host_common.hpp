@@ -4,7 +4,7 @@
 #include <cstdint>
 #include <vector>
 
-#include "../../../include/codag.h"
+#include "../../../include/codag_format.h"
 
 namespace codag_host {
 

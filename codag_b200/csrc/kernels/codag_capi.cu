@@ -623,11 +623,18 @@ extern "C" codag_status codag_decompress_rlev2_noalloc(const uint8_t* d_comp, ui
                                                        uint64_t n_chunks, uint64_t chunk_bytes, int elem_bytes,
                                                        uint8_t* d_out, uint64_t out_bytes, int32_t* d_chunk_status,
                                                        codag_stream_t stream) {
+  if (!d_comp || !d_blk_off || !d_col_len || (!d_out && out_bytes) || !valid_elem(elem_bytes) || chunk_bytes == 0 ||
+      chunk_bytes % static_cast<uint64_t>(elem_bytes) || chunk_bytes >= (1ull << 31))
+    return CODAG_EINVAL;  // the checks of dispatch_rle, made before the capacity check
   if (n_chunks > CODAG_NOALLOC_MAX_CHUNKS) return CODAG_ELIMIT;
   if (n_chunks == 0) return CODAG_OK;
   void* ws = nullptr;
   const codag_status st = noalloc_scratch(&ws);
   if (st != CODAG_OK) return st;
+  // The two-pass launch takes a workspace only when it is large and 256-byte aligned enough
+  // (launch_rle_out); both hold by construction, and if either did not, this call reports it
+  // instead of quietly decoding in one pass.
+  if ((reinterpret_cast<uintptr_t>(ws) & 255u) != 0 || kNoAllocScratchBytes < rle_ws_bytes(n_chunks)) return CODAG_ECUDA;
   return dispatch_rle<CODAG_CODEC_RLEV2>(d_comp, comp_bytes, d_blk_off, d_col_len, n_chunks, chunk_bytes, elem_bytes,
                                          d_out, out_bytes, d_chunk_status, ws, kNoAllocScratchBytes,
                                          reinterpret_cast<cudaStream_t>(stream));

@@ -24,6 +24,7 @@
 // elements per warp store.
 // Element arithmetic is modulo 2^(8*E), keeping the reference's quirks (oracle/oracle.c).
 #pragma once
+#include "../rlev2_widths.h"
 #include "device_common.cuh"
 
 namespace codag_dev {
@@ -52,15 +53,6 @@ __device__ __forceinline__ void put_elem(OUT& o, uint32_t idx, uint64_t v) {
 template <int E, class OUT>
 __device__ __forceinline__ uint64_t get_elem(const OUT& o, uint32_t idx) {
   return o.template get<E>(idx * static_cast<uint32_t>(E));
-}
-
-// bit width of a 5-bit width code (include/rlev2/utils.h:28)
-__host__ __device__ __forceinline__ uint32_t v2_width(uint32_t c) {
-  return c < 24 ? c + 1 : (c < 28 ? 2 * c - 22 : 8 * c - 184);
-}
-// smallest representable width >= b, for b in 0..64 (utils.h:42-48)
-__host__ __device__ __forceinline__ uint32_t v2_closest(uint32_t b) {
-  return b <= 24 ? (b ? b : 1u) : (b <= 32 ? (b + 1) & ~1u : (b + 7) & ~7u);
 }
 
 // LEB128 payload of the first `len` bytes of a little-endian window (len 1..8)

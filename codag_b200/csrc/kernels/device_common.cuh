@@ -6,7 +6,7 @@
 //            for the slots ahead of its read position and waits on each slot's mbarrier
 //            (bounded, see wait_slot) before reading it.  This replaces CODAG's
 //            warp-cooperative refill (include/common_warp.h:730-950) and its spin queues
-//            (common_warp.h:72-372).  No copy uses .multicast::cluster.
+//            (common_warp.h:72-372).  Every copy is a plain single-CTA bulk copy.
 //   OutRing  a shared-memory staging ring for decoded bytes, drained to global memory in
 //            fixed-size pieces with coalesced 16-byte vector stores.
 //
@@ -56,7 +56,7 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-// 1-D bulk copy global -> shared, completion counted on `bar` (no multicast).
+// 1-D bulk copy global -> shared, completion counted on `bar` (this CTA only).
 __device__ __forceinline__ void bulk_g2s(void* smem_dst, const void* gsrc, uint32_t bytes, uint64_t* bar) {
   asm volatile(
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(

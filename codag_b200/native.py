@@ -1,7 +1,9 @@
-"""ctypes binding of the C ABI in include/codag.h (libcodag_b200.so, built in-tree).
+"""ctypes bindings of the two in-tree libraries.
 
-The library is the product: every decode call goes to its CUDA kernels.  Loading fails
-loudly when the library has not been built; there is no Python or CPU fallback.
+libcodag_b200.so (include/codag.h) is the product: every decode call goes to its CUDA
+kernels.  libcodag_fmt.so (include/codag_format.h) holds the host-side format producers and
+seeded generators, and loads without the decoders.  Loading fails loudly when a library has
+not been built; there is no Python or CPU fallback.
 """
 from __future__ import annotations
 
@@ -11,6 +13,7 @@ from pathlib import Path
 import numpy as np
 
 LIB_PATH = Path(__file__).resolve().parent / "libcodag_b200.so"
+FMT_LIB_PATH = Path(__file__).resolve().parent / "libcodag_fmt.so"
 
 OK, EINVAL, ECORRUPT, ETIMEOUT, ECUDA, ENOMEM, ELIMIT = 0, 1, 2, 3, 4, 5, 6
 STATUS_NAMES = {OK: "OK", EINVAL: "EINVAL", ECORRUPT: "ECORRUPT", ETIMEOUT: "ETIMEOUT", ECUDA: "ECUDA", ENOMEM: "ENOMEM",
@@ -18,12 +21,15 @@ STATUS_NAMES = {OK: "OK", EINVAL: "EINVAL", ECORRUPT: "ECORRUPT", ETIMEOUT: "ETI
 NOALLOC_MAX_CHUNKS = 512  # CODAG_NOALLOC_MAX_CHUNKS
 RLEV1, RLEV2, DEFLATE = 0, 1, 2
 
-# every symbol declared in include/codag.h
+# every symbol declared in include/codag.h (libcodag_b200.so)
 EXPORTS = (
     "codag_decompress_rlev1", "codag_decompress_rlev2", "codag_decompress_deflate", "codag_workspace_bytes",
     "codag_decompress_rlev2_noalloc",
     "codag_set_tune", "codag_get_tune", "codag_set_wait_limit", "codag_selftest_wait_timeout",
     "codag_batch_plan", "codag_batch_run", "codag_batch_destroy", "codag_batch_launch",
+)
+# every symbol declared in include/codag_format.h (libcodag_fmt.so)
+FMT_EXPORTS = (
     "codag_hbuf_free", "codag_encode_rlev1", "codag_encode_rlev2", "codag_encode_deflate", "codag_encode_one",
     "codag_encode_set",
     "codag_gen_rlev1_column", "codag_gen_rlev2_column", "codag_gen_text",
@@ -55,6 +61,7 @@ CHUNK_DESC_DTYPE = np.dtype([("comp_off", "<u8"), ("out_off", "<u8"), ("comp_len
 assert CHUNK_DESC_DTYPE.itemsize == C.sizeof(ChunkDesc) == 32
 
 _lib = None
+_fmt = None
 
 
 def lib() -> C.CDLL:
@@ -87,6 +94,19 @@ def lib() -> C.CDLL:
     for name in ("codag_set_tune", "codag_get_tune", "codag_set_wait_limit", "codag_selftest_wait_timeout",
                  "codag_batch_plan", "codag_batch_run", "codag_batch_destroy", "codag_batch_launch"):
         getattr(L, name).restype = i32
+    _lib = L
+    return L
+
+
+def fmt_lib() -> C.CDLL:
+    """The loaded format library (raises if it was not built)."""
+    global _fmt
+    if _fmt is not None:
+        return _fmt
+    if not FMT_LIB_PATH.exists():
+        raise RuntimeError(f"{FMT_LIB_PATH} is missing: run `python -m codag_b200.build`")
+    L = C.CDLL(str(FMT_LIB_PATH))
+    u64, i32, vp = C.c_uint64, C.c_int32, C.c_void_p
     L.codag_hbuf_free.argtypes = [C.POINTER(HBuf)]
     L.codag_hbuf_free.restype = None
     enc = [vp, u64, u64, C.c_int, C.POINTER(HBuf), C.POINTER(HBuf), C.POINTER(HBuf)]
@@ -104,7 +124,7 @@ def lib() -> C.CDLL:
         getattr(L, name).restype = None
     L.codag_gen_text.argtypes = [u64, u64, vp]
     L.codag_gen_text.restype = None
-    _lib = L
+    _fmt = L
     return L
 
 
@@ -121,7 +141,7 @@ def _take(b: HBuf, dtype=np.uint8) -> np.ndarray:
             C.memmove(a.ctypes.data, b.data, b.bytes)
         return a.view(dtype)
     finally:
-        lib().codag_hbuf_free(C.byref(b))
+        fmt_lib().codag_hbuf_free(C.byref(b))
 
 
 def _ptr(a: np.ndarray) -> int:
@@ -135,7 +155,7 @@ def encode_rlev1(data: np.ndarray, chunk_bytes: int = 131072, elem_bytes: int = 
     """CODAG RLE v1 layout: (blob=[u64 size][streams], blk_off[n+1], col_len[n])."""
     raw = np.ascontiguousarray(data).view(np.uint8).reshape(-1)
     b1, b2, b3 = HBuf(), HBuf(), HBuf()
-    check("codag_encode_rlev1", lib().codag_encode_rlev1(_ptr(raw), raw.nbytes, chunk_bytes, elem_bytes,
+    check("codag_encode_rlev1", fmt_lib().codag_encode_rlev1(_ptr(raw), raw.nbytes, chunk_bytes, elem_bytes,
                                                         C.byref(b1), C.byref(b2), C.byref(b3)))
     return _take(b1), _take(b2, np.uint64), _take(b3, np.uint64)
 
@@ -144,7 +164,7 @@ def encode_rlev2(data: np.ndarray, chunk_bytes: int = 131072, elem_bytes: int = 
     """CODAG RLE v2 layout: (comp, blk_off[n+1] with blk_off[n] = size, col_len[n])."""
     raw = np.ascontiguousarray(data).view(np.uint8).reshape(-1)
     b1, b2, b3 = HBuf(), HBuf(), HBuf()
-    check("codag_encode_rlev2", lib().codag_encode_rlev2(_ptr(raw), raw.nbytes, chunk_bytes, elem_bytes,
+    check("codag_encode_rlev2", fmt_lib().codag_encode_rlev2(_ptr(raw), raw.nbytes, chunk_bytes, elem_bytes,
                                                         C.byref(b1), C.byref(b2), C.byref(b3)))
     return _take(b1), _take(b2, np.uint64), _take(b3, np.uint64)
 
@@ -154,7 +174,7 @@ def encode_deflate(data: np.ndarray, chunk_bytes: int = 131072, level: int = 6, 
     """CODAG Deflate layout: (comp, blk_offset[n+2] = [size, 0, cum...], col_len[n])."""
     raw = np.ascontiguousarray(data).view(np.uint8).reshape(-1)
     b1, b2, b3 = HBuf(), HBuf(), HBuf()
-    check("codag_encode_deflate", lib().codag_encode_deflate(_ptr(raw), raw.nbytes, chunk_bytes, level,
+    check("codag_encode_deflate", fmt_lib().codag_encode_deflate(_ptr(raw), raw.nbytes, chunk_bytes, level,
                                                             int(zlib_wrapper), int(require_no_stored),
                                                             C.byref(b1), C.byref(b2), C.byref(b3)))
     return _take(b1), _take(b2, np.uint64), _take(b3, np.uint64)
@@ -163,7 +183,7 @@ def encode_deflate(data: np.ndarray, chunk_bytes: int = 131072, level: int = 6, 
 def encode_one(codec: int, data: np.ndarray, elem_bytes: int = 8, level: int = 6) -> np.ndarray:
     raw = np.ascontiguousarray(data).view(np.uint8).reshape(-1)
     b = HBuf()
-    check("codag_encode_one", lib().codag_encode_one(codec, _ptr(raw), raw.nbytes, elem_bytes, level, C.byref(b)))
+    check("codag_encode_one", fmt_lib().codag_encode_one(codec, _ptr(raw), raw.nbytes, elem_bytes, level, C.byref(b)))
     return _take(b)
 
 
@@ -182,7 +202,7 @@ def encode_set(src: np.ndarray, in_off: np.ndarray, in_len: np.ndarray, codecs: 
     descs = np.zeros(n, dtype=CHUNK_DESC_DTYPE)
     b = HBuf()
     ob = C.c_uint64()
-    check("codag_encode_set", lib().codag_encode_set(_ptr(src), _ptr(in_off), _ptr(in_len), _ptr(codecs),
+    check("codag_encode_set", fmt_lib().codag_encode_set(_ptr(src), _ptr(in_off), _ptr(in_len), _ptr(codecs),
                                                     _ptr(elem_bytes), n, level, descs.ctypes.data, C.byref(b),
                                                     C.byref(ob)))
     return _take(b), descs, int(ob.value)
@@ -190,19 +210,19 @@ def encode_set(src: np.ndarray, in_off: np.ndarray, in_len: np.ndarray, codecs: 
 
 def gen_rlev1_column(n: int, seed: int, elem_bytes: int = 8) -> np.ndarray:
     out = np.empty(n * elem_bytes, dtype=np.uint8)
-    lib().codag_gen_rlev1_column(n, seed, elem_bytes, _ptr(out))
+    fmt_lib().codag_gen_rlev1_column(n, seed, elem_bytes, _ptr(out))
     return out
 
 
 def gen_rlev2_column(n: int, seed: int, elem_bytes: int = 8) -> np.ndarray:
     out = np.empty(n * elem_bytes, dtype=np.uint8)
-    lib().codag_gen_rlev2_column(n, seed, elem_bytes, _ptr(out))
+    fmt_lib().codag_gen_rlev2_column(n, seed, elem_bytes, _ptr(out))
     return out
 
 
 def gen_text(nbytes: int, seed: int) -> np.ndarray:
     out = np.empty(nbytes, dtype=np.uint8)
-    lib().codag_gen_text(nbytes, seed, _ptr(out))
+    fmt_lib().codag_gen_text(nbytes, seed, _ptr(out))
     return out
 
 

@@ -88,7 +88,12 @@ uint64_t codag_workspace_bytes(int codec, uint64_t n_chunks);
  * device that loads the library holds until the process exits.
  *   - n_chunks above CODAG_NOALLOC_MAX_CHUNKS returns CODAG_ELIMIT (split the request).
  *   - The first call on a device looks up the array's device address on that device
- *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *     (cudaGetSymbolAddress); make that first call before any stream capture.  The address
+ *     is kept per device number for the device's primary context (the runtime's own
+ *     context); it is not valid after cudaDeviceReset, nor in another context made current
+ *     on that device.
+ *   - Arguments are checked as codag_decompress_rlev2 checks them (CODAG_EINVAL), before
+ *     the chunk-count limit.
  *   - Every call shares the one array and leaves its contents behind.  Calls whose work
  *     overlaps on the GPU (different streams, or different host threads) race on it:
  *     order them on one stream or with events.
@@ -188,50 +193,6 @@ codag_status codag_batch_launch(const codag_chunk_desc *d_descs, const uint32_t 
                                 uint32_t *d_queue, const codag_tune *tune, const uint8_t *d_comp,
                                 uint64_t comp_bytes, uint8_t *d_out, uint64_t out_bytes,
                                 int32_t *d_status, codag_stream_t stream);
-
-/* --- host-side format producers (CPU; used by the CLIs, tests and benchmarks) ---------- */
-typedef struct {
-    uint8_t *data;
-    uint64_t bytes;
-} codag_hbuf; /* malloc'd by the library; release with codag_hbuf_free */
-void codag_hbuf_free(codag_hbuf *b);
-
-/* CODAG's RLE v1 layout (include/rlev1/rlev1.h:103-192): blob = [u64 in_bytes][streams],
- * blk_off = n_pad+1 u64 (stream i at blob+8+blk_off[i], 4-byte aligned), col_len = n_pad u64,
- * n_pad = ceil(in_bytes/(chunk*32))*32 chunks over the zero-padded input. */
-codag_status codag_encode_rlev1(const uint8_t *in, uint64_t in_bytes, uint64_t chunk_bytes,
-                                int elem_bytes, codag_hbuf *blob, codag_hbuf *blk_off,
-                                codag_hbuf *col_len);
-/* CODAG's RLE v2 layout (include/rlev2/encoder_trans.h:482-564): streams at 128-byte aligned
- * blk_off[i]; blk_off has n_pad+1 entries with blk_off[n_pad] = in_bytes; col_len n_pad. */
-codag_status codag_encode_rlev2(const uint8_t *in, uint64_t in_bytes, uint64_t chunk_bytes,
-                                int elem_bytes, codag_hbuf *comp, codag_hbuf *blk_off,
-                                codag_hbuf *col_len);
-/* CODAG's Deflate layout (deflate_compressor.py:44-125): input zero padded to a multiple of
- * chunk_bytes; comp = zlib streams each padded to 8 bytes; blk_offset = n+2 u64
- * [in_bytes, 0, cum_1 .. cum_n]; col_len = n padded sizes.  zlib_wrapper=1 writes RFC 1950
- * streams (CODAG's format), 0 raw Deflate.  Fails with CODAG_EINVAL if require_no_stored and
- * zlib emitted a stored block. */
-codag_status codag_encode_deflate(const uint8_t *in, uint64_t in_bytes, uint64_t chunk_bytes,
-                                  int level, int zlib_wrapper, int require_no_stored,
-                                  codag_hbuf *comp, codag_hbuf *blk_offset, codag_hbuf *col_len);
-/* One stream of a single buffer (the batched workload's per-chunk files). */
-codag_status codag_encode_one(int codec, const uint8_t *in, uint64_t in_bytes, int elem_bytes,
-                              int level, codag_hbuf *stream);
-
-/* A set of n independent files, file i = in[in_off[i] .. +in_len[i]), each encoded as ONE
- * stream of codecs[i] (Deflate: zlib level `level` with the 2-byte zlib wrapper; RLE:
- * elem_bytes[i]-wide values) and packed for codag_batch_plan: streams 16-byte aligned in
- * `comp`, outputs 256-byte aligned in an output buffer of *out_bytes; descs[i] is filled.
- * OpenMP over files. */
-codag_status codag_encode_set(const uint8_t *in, const uint64_t *in_off, const uint64_t *in_len,
-                              const uint8_t *codecs, const uint8_t *elem_bytes, uint64_t n, int level,
-                              codag_chunk_desc *descs, codag_hbuf *comp, uint64_t *out_bytes);
-
-/* Seeded synthetic columns (splitmix64/xoshiro256**). */
-void codag_gen_rlev1_column(uint64_t n, uint64_t seed, int elem_bytes, uint8_t *out);
-void codag_gen_rlev2_column(uint64_t n, uint64_t seed, int elem_bytes, uint8_t *out);
-void codag_gen_text(uint64_t bytes, uint64_t seed, uint8_t *out);
 
 #ifdef __cplusplus
 }

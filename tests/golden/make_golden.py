@@ -1,12 +1,12 @@
 """Regenerates the golden files of tests/golden from CODAG's own Python compressor.
 
-Runs only where the CODAG tree is available (default /root/reference, or $CODAG_REF).
+Runs only where the CODAG tree is available: give it with --ref or $CODAG_REFERENCE_DIR.
 deflate_compressor.py imports `zstandard` at module level without using it on this path,
 and writes to a hard-coded directory; the script stubs the first and redirects the second
 into this folder, then calls CODAG's zlib_chunk_compress (deflate_compressor.py:44-125)
 on a seeded text sample.  The tests compare our layout writer against these files.
 
-    python tests/golden/make_golden.py
+    CODAG_REFERENCE_DIR=<CODAG tree> python tests/golden/make_golden.py
 """
 import builtins
 import os
@@ -18,10 +18,13 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[1]
-REF = Path(os.environ.get("CODAG_REF", "/root/reference"))
 
 
 def main() -> None:
+    ref = sys.argv[sys.argv.index("--ref") + 1] if "--ref" in sys.argv else os.environ.get("CODAG_REFERENCE_DIR")
+    if not ref:
+        sys.exit("give the CODAG source tree with --ref or CODAG_REFERENCE_DIR")
+    REF = Path(ref)
     sys.path.insert(0, str(REPO))
     from codag_b200 import native
 

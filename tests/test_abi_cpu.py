@@ -1,24 +1,45 @@
-"""The C ABI library loads and exports every symbol include/codag.h declares; argument
-checks that need no GPU return CODAG_EINVAL.  No decode calls here (no GPU)."""
+"""The C ABI libraries load and export every symbol their headers declare (include/codag.h:
+libcodag_b200.so; include/codag_format.h: libcodag_fmt.so), the decoder library holds no
+format producer and the format library no CUDA; argument checks that need no GPU return
+CODAG_EINVAL.  No decode calls here (no GPU)."""
 import ctypes as C
 import re
 from pathlib import Path
 
-HEADER = Path(__file__).resolve().parents[1] / "include" / "codag.h"
+INCLUDE = Path(__file__).resolve().parents[1] / "include"
 
 
-def declared_functions():
-    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+def declared_functions(header):
+    text = re.sub(r"/\*.*?\*/", "", (INCLUDE / header).read_text(), flags=re.S)
     return sorted(set(re.findall(r"\b(codag_[a-z0-9_]+)\s*\(", text)))
 
 
 def test_exports_every_declared_symbol(native):
-    names = declared_functions()
-    assert len(names) >= 18
+    names = declared_functions("codag.h")
+    assert len(names) >= 13
     lib = native.lib()
     missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, missing
     assert set(names) == set(native.EXPORTS)
+
+
+def test_format_library_exports_every_declared_symbol(native):
+    names = declared_functions("codag_format.h")
+    assert len(names) >= 9
+    lib = native.fmt_lib()
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) == set(native.FMT_EXPORTS)
+
+
+def test_libraries_are_separate(native):
+    """The format library loads without CUDA (a CPU-only caller, such as the timed CPU
+    decoder, never maps the decoders), and the decoder library carries no producer."""
+    import subprocess
+    deps = subprocess.run(["ldd", str(native.FMT_LIB_PATH)], capture_output=True, text=True).stdout
+    assert "libcudart" not in deps and "libcuda." not in deps
+    dec = subprocess.run(["nm", "-D", "--defined-only", str(native.LIB_PATH)], capture_output=True, text=True).stdout
+    assert "codag_encode_set" not in dec and "codag_gen_text" not in dec
 
 
 def test_argument_validation_without_gpu(native):

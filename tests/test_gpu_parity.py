@@ -17,6 +17,8 @@ def _bytes_of(values, e):
 
 def _t(cuda, a, dtype=None):
     a = np.ascontiguousarray(a)
+    if not a.flags.writeable:  # torch.from_numpy warns on read-only arrays
+        a = a.copy()
     if a.dtype == np.uint64:
         a = a.view(np.int64)
     return cuda.from_numpy(a).to("cuda")

@@ -5,7 +5,8 @@ caller workspace.
 
 Its output must equal codag_decompress_rlev2's on the same input, byte for byte, over two
 calls in a row with different inputs: the second call reuses the scratch the first one
-left behind.  This file is collected last so that a run stopping at the first failure has
+left behind.  The entry point returns an error rather than decoding in one pass when its
+scratch could not be used, so a match here is a match of the two-pass decode.  This file is collected last so that a run stopping at the first failure has
 already run every other test.
 """
 import ctypes as C
@@ -25,9 +26,20 @@ def _column(n_values, seed, e):
 def test_rejects_more_chunks_than_the_scratch_holds(native):
     lib = native.lib()
     n = native.NOALLOC_MAX_CHUNKS + 1
-    # the size check comes before any CUDA call, so it runs without a GPU too
+    # the argument and size checks come before any CUDA call, so they run without a GPU too
     assert lib.codag_decompress_rlev2_noalloc(1, 1, 1, 1, n, CHUNK, 8, 1, 1, None, None) == native.ELIMIT
     assert lib.codag_decompress_rlev2_noalloc(1, 1, 1, 1, 0, CHUNK, 8, 1, 1, None, None) == native.OK
+
+
+def test_checks_arguments_like_the_workspace_call(native):
+    """Bad pointers and element widths give CODAG_EINVAL before the chunk-count limit is
+    looked at, and with no chunks at all, as codag_decompress_rlev2 does."""
+    lib = native.lib()
+    for n in (0, 1, native.NOALLOC_MAX_CHUNKS + 1):
+        assert lib.codag_decompress_rlev2_noalloc(None, 1, 1, 1, n, CHUNK, 8, 1, 1, None, None) == native.EINVAL
+        assert lib.codag_decompress_rlev2_noalloc(1, 1, 1, 1, n, CHUNK, 3, 1, 1, None, None) == native.EINVAL
+        assert lib.codag_decompress_rlev2_noalloc(1, 1, 1, 1, n, CHUNK + 4, 8, 1, 1, None, None) == native.EINVAL
+        assert lib.codag_decompress_rlev2(None, 1, 1, 1, n, CHUNK, 8, 1, 1, None, None, 0, None) == native.EINVAL
 
 
 def _decode_both(cuda, data, e):
