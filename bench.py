@@ -2,21 +2,28 @@
 """Benchmark of the chunked decompressors on one node (one process per GPU).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload rlev2|rlev1|rlev1x128|deflate|batched]
+                    [--workload batched|rlev2|rlev1|rlev1x128|deflate|serving] [--no-extras]
 
-Default workload (rlev2): CODAG's RLE v2 configuration -- 134,217,728 int64 values (1 GiB)
-of seeded synthetic segments in 8,192 chunks of 128 KiB, decoded by one plain per-file
-launch per step.  Inputs (compressed + decompressed, about 1.2 GB) exceed the 126 MB L2,
-so no flush is needed between steps.  N>1: every rank decodes its own instance (weak
-scaling, no collective on the data path; timing is the max over ranks).
+Default workload (batched): CODAG's batched configuration -- 20,000 independently compressed
+files, decompressed size log-uniform 4 KiB-1 MiB, 40% Deflate / 30% RLE v1 / 30% RLE v2, RLE
+values u32 or u64 (50/50), about 3.8 GB decompressed -- decoded per step by one persistent
+launch replayed from a CUDA graph (`value`), and compared with the plain per-file path (one
+C-ABI call per file, the only way CODAG's kernels can decode such a set): `plain_per_file`
+and `batched_over_plain`.  With one GPU the same line also carries, under `configs`, the
+per-codec configurations (RLE v2 1 GiB, RLE v1 8 MiB and 1 GiB, Deflate 1 GiB text) with
+their own roofline, e2e and CPU baseline, and a short serving sweep (Poisson arrivals at two
+rates, p50/p99 latency).  Inputs exceed the 126 MB L2, so no flush is needed between steps.
+N>1: every rank decodes its own instance (weak scaling, no collective on the data path;
+timing is the max over ranks); the extra configurations run at N=1 only.
 
-Prints one JSON line (rank 0).  `value` is decompressed GB/s with inputs resident in HBM;
-`e2e` is the same metric through the host-buffer API (api.HostPipeline: pinned H2D of the
-streams and metadata, decode, D2H of the output, every step, overlapped by chunk groups); `roofline` relates the decode kernel's
-algorithmic bytes (compressed bytes read + decompressed bytes written) to the measured
-HBM copy bandwidth; `cpu_baseline` is the CPU oracle (OpenMP over chunks) on a bounded
-sample of the same workload.  --impl reference times that CPU decoder as the reference arm
-(CODAG's own decoders exist only as GPU kernels; the oracle restates them on the CPU).
+`value` is decompressed GB/s with inputs resident in HBM; `e2e` is the same metric through the
+host-buffer API with every host-to-device copy of the inputs and device-to-host copy of the
+outputs in the timed region; `roofline` relates the decode kernel's algorithmic bytes
+(compressed bytes read + decompressed bytes written) to the measured HBM copy bandwidth;
+`cpu_baseline` is the CPU decoder (OpenMP over chunks or files) on a bounded sample.
+--impl reference times that CPU decoder on the whole workload as the reference arm (CODAG's
+own decoders exist only as GPU kernels; the oracle restates them on the CPU).  The reference
+arm loads only the format library (libcodag_fmt.so) and the oracle, never the decoders.
 """
 from __future__ import annotations
 
@@ -38,6 +45,8 @@ sys.path.insert(0, str(ROOT))
 
 CH = 131072
 SEED = 20260101
+METRIC = "decompressed GB/s on 1 B200, batched vs plain per-file; p50/p99 request latency"
+DATA = "synthetic (seeded generators standing in for CODAG's datasets)"
 WORKLOADS = {
     "rlev2": dict(codec=1, n=134_217_728, elem=8, desc="ORC RLE v2, 134,217,728 int64 (1 GiB), 8192 x 128 KiB chunks"),
     "rlev1": dict(codec=0, n=1_048_576, elem=8, desc="ORC RLE v1, 1,048,576 uint64 (8 MiB), 64 x 128 KiB chunks"),
@@ -45,6 +54,7 @@ WORKLOADS = {
     "deflate": dict(codec=2, n=1 << 30, elem=1, desc="Deflate (zlib level 6), 1 GiB Zipf text, 8192 x 128 KiB chunks"),
 }
 KERNEL_NAMES = {0: "k_rle_plain<.., RLEV1>", 1: "k_rle_plain<.., RLEV2>", 2: "k_inflate_plain"}
+EXTRA_CONFIGS = ("rlev2", "rlev1", "rlev1x128", "deflate")
 
 
 def peaks():
@@ -104,7 +114,7 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-# --- workload construction (product format producers) -------------------------------------------
+# --- workload construction (format library only) ------------------------------------------------
 def make_file(workload: str, rank: int, n_values: int | None = None):
     from codag_b200 import native as nat
     w = dict(WORKLOADS[workload])
@@ -124,19 +134,22 @@ def make_file(workload: str, rank: int, n_values: int | None = None):
     return dict(col=txt, comp=comp, off=bo[1:], ln=cl)
 
 
+def _oracle_args(f, codec: int, elem: int, n: int):
+    if codec == 2:
+        comp_off, comp_len, wrapper = f["off"][:n], np.diff(f["off"][:n + 1]), [2] * n
+    else:
+        comp_off, comp_len, wrapper = f["off"][:n], f["ln"][:n], [0] * n
+    out = np.empty(n * CH, np.uint8)
+    return (f["comp"], comp_off, comp_len, out, np.arange(n, dtype=np.uint64) * CH, [CH] * n, [CH] * n,
+            [codec] * n, [elem] * n, wrapper)
+
+
 def cpu_sample(f, codec: int, elem: int, max_chunks: int):
-    """Oracle decode of the first max_chunks chunks on all host threads; returns (GB/s, threads, desc)."""
+    """CPU decoder (the oracle, OpenMP over chunks) on the first max_chunks chunks with all host
+    threads; returns (GB/s, threads, description)."""
     from oracle import oracle_py
     n = min(max_chunks, f["ln"].size)
-    if codec == 2:
-        comp_off, comp_len = f["off"][:n], np.diff(f["off"][:n + 1])
-        wrapper = [2] * n
-    else:
-        comp_off, comp_len = f["off"][:n], f["ln"][:n]
-        wrapper = [0] * n
-    out = np.empty(n * CH, np.uint8)
-    args = (f["comp"], comp_off, comp_len, out, np.arange(n, dtype=np.uint64) * CH, [CH] * n, [CH] * n,
-            [codec] * n, [elem] * n, wrapper)
+    args = _oracle_args(f, codec, elem, n)
     oracle_py.decode_batch(*args)  # warm-up
     times = []
     for _ in range(3):
@@ -148,21 +161,13 @@ def cpu_sample(f, codec: int, elem: int, max_chunks: int):
     return n * CH / t / 1e9, oracle_py.max_threads(), f"{n} chunks x 128 KiB ({n * CH / 2**20:.0f} MiB), median of 3"
 
 
-# --- arms ------------------------------------------------------------------------------------------
+# --- reference arm (CPU decoder of the path, whole workload per step) -----------------------------
 def run_reference(args):
-    """CPU decoder of the path (oracle port, OpenMP over chunks) on a bounded sample per step."""
+    from oracle import oracle_py
     w = WORKLOADS[args.workload]
     f = make_file(args.workload, 0, args.n_values)
-    sample = 1024 if w["codec"] != 2 else 256
-    from oracle import oracle_py
-    n = min(sample, f["ln"].size)
-    if w["codec"] == 2:
-        comp_off, comp_len, wrapper = f["off"][:n], np.diff(f["off"][:n + 1]), [2] * n
-    else:
-        comp_off, comp_len, wrapper = f["off"][:n], f["ln"][:n], [0] * n
-    out = np.empty(n * CH, np.uint8)
-    a = (f["comp"], comp_off, comp_len, out, np.arange(n, dtype=np.uint64) * CH, [CH] * n, [CH] * n,
-         [w["codec"]] * n, [w["elem"]] * n, wrapper)
+    n = f["ln"].size
+    a = _oracle_args(f, w["codec"], w["elem"], n)
     for _ in range(args.warmup):
         oracle_py.decode_batch(*a)
     t0 = time.perf_counter()
@@ -170,29 +175,34 @@ def run_reference(args):
         st = oracle_py.decode_batch(*a)
     dt = time.perf_counter() - t0
     assert not st.any()
-    gbs = args.steps * n * CH / dt / 1e9
+    out_bytes = f["col"].size
+    ok = bool(np.array_equal(a[3][:out_bytes], f["col"].view(np.uint8)))
+    gbs = args.steps * out_bytes / dt / 1e9
     threads = oracle_py.max_threads()
-    desc = f"{n} chunks x 128 KiB of the workload per step ({n * CH / 2**20:.0f} MiB)"
+    desc = f"all {n} chunks of the workload per step ({out_bytes / 2**20:.0f} MiB decompressed)"
     line = {"metric": "decompressed GB/s", "value": round(gbs, 3), "unit": "GB/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 3),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8" if w["codec"] == 2 else "int64",
-            "data": "synthetic (seeded generators standing in for CODAG's datasets)",
-            "config": {"workload": w["desc"], "chunk_bytes": CH, "sample": desc},
-            "impl": "reference",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u8" if w["codec"] == 2 else "int64", "data": DATA,
+            "config": {"workload": w["desc"], "chunk_bytes": CH, "n_chunks": n, "out_bytes": out_bytes},
+            "bit_exact": ok, "impl": "reference",
             "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port", "sample": desc},
             "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args, rank: int, world: int, local: int):
+# --- our arm, one codec configuration -----------------------------------------------------------
+def measure_codec(workload: str, args, rank: int, world: int, local: int, steps: int, warmup: int,
+                  clocks_on: bool = True):
+    """Times one per-codec configuration; returns its JSON line (rank 0) or None."""
     import torch
     import torch.distributed as dist
     from codag_b200 import api, native as nat
 
     torch.cuda.set_device(local)
-    w = WORKLOADS[args.workload]
+    w = WORKLOADS[workload]
     codec, e = w["codec"], w["elem"]
-    f = make_file(args.workload, rank, args.n_values)
+    f = make_file(workload, rank, args.n_values)
     n = f["ln"].size
     out_bytes = f["col"].size
     comp_bytes = f["comp"].size
@@ -207,32 +217,31 @@ def run_ours(args, rank: int, world: int, local: int):
     d_out = torch.empty(n * CH, dtype=torch.uint8, device=dev)
     d_st = torch.zeros(n, dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream()
-    # two-pass RLE scratch (resident); --rle-passes 1 decodes in a single pass without it
     d_ws = api.workspace(codec, n, dev) if codec != 2 and args.rle_passes == 2 else None
 
-    def launch(comp=d_comp, off=d_off, ln=d_len, out=d_out, obytes=None):
+    def launch():
         if codec == 0:
-            api.decompress_rlev1(comp, off, ln, CH, e, out, obytes, d_st, stream, ws=d_ws)
+            api.decompress_rlev1(d_comp, d_off, d_len, CH, e, d_out, None, d_st, stream, ws=d_ws)
         elif codec == 1:
-            api.decompress_rlev2(comp, off, ln, CH, e, out, obytes, d_st, stream, ws=d_ws)
+            api.decompress_rlev2(d_comp, d_off, d_len, CH, e, d_out, None, d_st, stream, ws=d_ws)
         else:
-            api.decompress_deflate(comp, off, CH, out, 2, obytes, d_st, stream)
+            api.decompress_deflate(d_comp, d_off, CH, d_out, 2, None, d_st, stream)
 
     if args.tune:
         nat.set_tune(codec, *[int(x) for x in args.tune.split(",")])
     elif args.autotune:
         from codag_b200 import tuning
         # the best shape depends on the chunk count (few chunks favour a CTA per chunk)
-        best, res = tuning.autotune(codec, launch, tag=f"plain-{n}chunks", use_cache=args.autotune == "cached",
-                                    verbose=rank == 0)
-    for _ in range(max(args.warmup, 3)):
+        tuning.autotune(codec, launch, tag=f"plain-{n}chunks", use_cache=args.autotune == "cached",
+                        verbose=rank == 0 and args.verbose)
+    for _ in range(max(warmup, 3)):
         launch()
     torch.cuda.synchronize()
     # correctness of the timed configuration (outside the timed region)
     ok = int((d_st != 0).sum().item()) == 0 and bool(torch.equal(d_out[:out_bytes], torch.from_numpy(f["col"]).to(dev)))
 
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    clocks = Clocks(local) if rank == 0 else None
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    clocks = Clocks(local) if rank == 0 and clocks_on else None
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -241,7 +250,7 @@ def run_ours(args, rank: int, world: int, local: int):
         time.sleep(0.3)
     t_all0, t_all1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t_all0.record(stream)
-    for i in range(args.steps):
+    for i in range(steps):
         ev[i][0].record(stream)
         launch()
         ev[i][1].record(stream)
@@ -270,7 +279,7 @@ def run_ours(args, rank: int, world: int, local: int):
     h_len = torch.from_numpy(len_np.view(np.int64)).pin_memory() if codec != 2 else None
     h_out = torch.empty(out_bytes, dtype=torch.uint8).pin_memory()
     pipe = api.HostPipeline(codec, CH, e, 2, groups=args.e2e_groups, device=dev)
-    e_steps = max(2, min(args.steps, 5))
+    e_steps = max(2, min(steps, 5))
     h2d_bytes = h_comp.numel() + 8 * h_off.numel() + (8 * h_len.numel() if codec != 2 else 0)
     pipe.run(h_comp, h_off, h_len, out_bytes, h_out, off_np, len_np)  # sizes the device buffers
     if world > 1:
@@ -288,45 +297,49 @@ def run_ours(args, rank: int, world: int, local: int):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_t = float(t.item())
     ok = ok and bool(torch.equal(h_out, torch.from_numpy(f["col"])))
+    del d_comp, d_off, d_len, d_out, d_st, d_ws, pipe
+    torch.cuda.empty_cache()
 
     if rank != 0:
-        return
+        return None
     peak, peak_kind = peaks()
     achieved = alg_bytes / per_launch / 1e9
-    launches = args.steps
-    value = world * out_bytes * args.steps / elapsed / 1e9
-    traffic = ncu_traffic(args.workload)
+    value = world * out_bytes * steps / elapsed / 1e9
     cpu = None
     if world == 1:
         gbs, threads, desc = cpu_sample(f, codec, e, 1024 if codec != 2 else 256)
         cpu = {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port", "sample": desc}
-    line = {
+    t = nat.get_tune(codec)
+    return {
         "metric": "decompressed GB/s", "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(elapsed / args.steps * 1e3, 4),
+        "steps": steps, "warmup": warmup, "ms_per_step": round(elapsed / steps * 1e3, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "u8" if codec == 2 else "int64",
-        "data": "synthetic (seeded generators standing in for CODAG's datasets)",
+        "dtype": "u8" if codec == 2 else "int64", "data": DATA,
         "config": {"workload": w["desc"] if not args.n_values else f"{w['desc']} resized to {args.n_values} values",
                    "chunk_bytes": CH, "n_chunks": n, "comp_bytes": comp_bytes,
                    "out_bytes": out_bytes, "l2": "inputs larger than L2 (no flush)",
                    "parallelism": f"{world} GPU(s), chunks per GPU independent",
-                   "tune": {k: getattr(nat.get_tune(codec), k)
-                            for k in ("warps_per_cta", "ring_slots", "lut_bits", "cta_per_chunk")}},
+                   "tune": {k: getattr(t, k) for k in ("warps_per_cta", "ring_slots", "lut_bits", "cta_per_chunk")}},
         "bit_exact": ok,
         "e2e": {"value": round(world * out_bytes * e_steps / e2e_t / 1e9, 2), "unit": "GB/s",
                 "h2d_bytes_per_step": int(h2d_bytes), "d2h_bytes_per_step": int(out_bytes)},
-        "gpu_launches": launches,
+        "gpu_launches": steps * (2 if codec != 2 and args.rle_passes == 2 else 1),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": ("k_rle_cta<RLEV1/RLEV2, E>" if codec != 2 and nat.get_tune(codec).cta_per_chunk
-                                else KERNEL_NAMES[codec]), "alg_bytes_per_launch": alg_bytes,
+                     "frac": round(achieved / peak, 4), "traffic": ncu_traffic(workload), "peak_kind": peak_kind,
+                     "kernel": ("k_rle_cta<RLEV1/RLEV2, E>" if codec != 2 and t.cta_per_chunk else KERNEL_NAMES[codec]),
+                     "alg_bytes_per_launch": alg_bytes,
                      "note": ("launch = header walk + expansion kernels of one call" if codec != 2 and args.rle_passes == 2
                               else "one kernel"),
                      "launch_ms": round(per_launch * 1e3, 4)},
         "cpu_baseline": cpu,
         "clocks": clk,
     }
-    print(json.dumps(line), flush=True)
+
+
+def _summary(line: dict) -> dict:
+    """The figures of a per-codec line kept under the headline's `configs`."""
+    keep = ("value", "unit", "ms_per_step", "bit_exact", "e2e", "roofline", "cpu_baseline", "clocks")
+    return {"workload": line["config"]["workload"], **{k: line[k] for k in keep}, "tune": line["config"]["tune"]}
 
 
 def main():
@@ -335,14 +348,16 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="rlev2", choices=sorted(WORKLOADS) + ["batched", "serving"])
+    ap.add_argument("--workload", default="batched", choices=["batched"] + sorted(WORKLOADS) + ["serving"])
+    ap.add_argument("--no-extras", dest="extras", action="store_false",
+                    help="batched: skip the per-codec configurations and the short serving sweep")
     ap.add_argument("--autotune", default="cached", choices=["cached", "search", ""],
                     help="pick the launch shape with the autotuner (cached result or a fresh search)")
     ap.add_argument("--rle-passes", type=int, default=1, choices=[1, 2],
                     help="RLE: 2 = header walk + expansion (with workspace), 1 = single pass")
     ap.add_argument("--tune", default="", help="explicit launch shape warps_per_cta,ring_slots,lut_bits[,cta_per_chunk]")
     ap.add_argument("--n-values", type=int, default=None,
-                    help="override the workload's element count (profiling cases; not a bench line)")
+                    help="override a codec workload's element count (profiling cases; not a bench line)")
     ap.add_argument("--n-files", type=int, default=None, help="batched: number of files (default 20,000)")
     ap.add_argument("--e2e-groups", type=int, default=8, help="e2e: chunk groups overlapped by the host pipeline")
     ap.add_argument("--per-file-sample", type=int, default=600,
@@ -352,6 +367,8 @@ def main():
     ap.add_argument("--pool-files", type=int, default=48, help="serving: distinct request files")
     ap.add_argument("--budget-gb", type=int, default=64, help="serving: output memory budget")
     ap.add_argument("--slots", type=int, default=4, help="serving: launches in flight")
+    ap.add_argument("--extra-steps", type=int, default=10, help="batched: timed steps of each extra configuration")
+    ap.add_argument("--verbose", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -376,12 +393,26 @@ def main():
     try:
         if args.workload == "batched":
             import bench_batched
-            bench_batched.main(args, rank, world, local)
+            line = bench_batched.main(args, rank, world, local)
+            if rank == 0 and line is not None and world == 1 and args.extras:
+                import bench_serving
+                configs = {}
+                for wl in EXTRA_CONFIGS:
+                    configs[wl] = _summary(measure_codec(wl, args, rank, world, local, args.extra_steps, 3,
+                                                         clocks_on=False))
+                configs["serving"] = bench_serving.short_sweep(args, local)
+                line["configs"] = configs
+                line["configs_note"] = ("per-codec configurations and a short serving sweep, timed in the same run "
+                                        f"({args.extra_steps} steps each; serving: 2 rates x 10 s)")
+            if line is not None:
+                print(json.dumps(line), flush=True)
         elif args.workload == "serving":
             import bench_serving
             bench_serving.main(args, rank, world, local)
         else:
-            run_ours(args, rank, world, local)
+            line = measure_codec(args.workload, args, rank, world, local, args.steps, args.warmup)
+            if line is not None:
+                print(json.dumps(line), flush=True)
     finally:
         if world > 1:
             import torch.distributed as dist

@@ -13,6 +13,33 @@ import json
 SEED = 20260105
 
 
+def short_sweep(args, local: int, rates=(500.0, 2000.0), duration: float = 10.0, pool_files: int = 24) -> dict:
+    """A short sweep for the default bench line: `rates` for `duration` seconds each over a
+    pool of `pool_files` files; returns decompressed GB/s and p50/p99 latency per rate."""
+    import torch
+    from codag_b200 import serving
+
+    torch.cuda.set_device(local)
+    pool = serving.build_pool(pool_files, SEED)
+    srv = serving.Server(pool, args.budget_gb << 30, slots=args.slots, device=f"cuda:{local}")
+    srv.run(serving.poisson_arrivals(50, 0.5, len(pool.files), 1))
+    rows = []
+    for k, rate in enumerate(rates):
+        arr = serving.poisson_arrivals(rate, duration, len(pool.files), SEED + 17 * k)
+        reqs = srv.run(arr, time_limit=duration * 3 + 30)
+        s = serving.summarize(reqs, pool, duration)
+        rows.append({"rate": rate, **{k2: (round(v, 3) if isinstance(v, float) else v) for k2, v in s.items()}})
+    sizes = [f.size for f in pool.files]
+    out = {"workload": f"serving: Poisson arrivals, {duration:g} s per rate, pool of {len(pool.files)} files "
+                       f"log-uniform 64 KiB-256 MiB (mean {sum(sizes) / len(sizes) / 1e6:.1f} MB), "
+                       "40/30/30 Deflate/RLE v1/RLE v2, 128 KiB chunks",
+           "budget_bytes": args.budget_gb << 30, "rates": rows, "bit_exact": all(r["bit_exact"] for r in rows),
+           "launches": srv.launches}
+    del srv, pool
+    torch.cuda.empty_cache()
+    return out
+
+
 def main(args, rank: int, world: int, local: int) -> None:
     import torch
     from codag_b200 import serving
