@@ -278,6 +278,71 @@ class BatchPlan:
             pass
 
 
+class BatchHostPipeline:
+    """Decodes a packed set of independent files (codag_batch_plan descriptors) from pinned host
+    memory into pinned host memory, overlapping the copies with the decode.
+
+    The files are split into `groups` of about equal decode cost (Deflate bytes weigh more),
+    each with its own persistent plan; group g's compressed bytes go up, its launch runs and
+    its outputs come down on stream g % streams, so one group's host-to-device copy, another
+    group's decode and a third group's device-to-host copy overlap, and the launches of
+    different groups overlap on the GPU as well (a launch ends with its longest file while the
+    next one fills the other SMs).  Files must be packed in index order, as pack_chunks and
+    codag_encode_set do, so each group's input and output are contiguous ranges.  Device
+    buffers and plans live as long as the pipeline; bytes between outputs are zero."""
+
+    def __init__(self, descs: np.ndarray, comp_bytes: int, out_bytes: int, groups: int = 6, streams: int = 3,
+                 shape: tuple | None = None, device="cuda"):
+        descs = np.ascontiguousarray(descs, dtype=native.CHUNK_DESC_DTYPE)
+        n = descs.size
+        self.dev = torch.device(device)
+        cost = descs["out_len"].astype(np.int64) + np.where(descs["codec"] == native.DEFLATE, 8, 1) * \
+            descs["comp_len"].astype(np.int64)
+        cum = np.cumsum(cost)
+        cuts = np.searchsorted(cum, np.linspace(0, cum[-1], min(groups, n) + 1)[1:-1], side="right")
+        bounds = np.unique(np.concatenate([[0], cuts, [n]]))
+        self.groups = []
+        for a, b in zip(bounds[:-1], bounds[1:]):
+            d = descs[a:b]
+            self.groups.append(dict(
+                a=int(a), b=int(b), plan=BatchPlan(d, *(shape or ())),
+                c0=int(d["comp_off"].min()), c1=int((d["comp_off"] + d["comp_len"]).max()),
+                o0=int(d["out_off"].min()), o1=int((d["out_off"] + d["out_len"]).max())))
+        self.d_comp = torch.empty(max(comp_bytes, 1), dtype=torch.uint8, device=self.dev)
+        self.d_out = torch.zeros(max(out_bytes, 1), dtype=torch.uint8, device=self.dev)
+        self.d_st = torch.zeros(max(n, 1), dtype=torch.int32, device=self.dev)
+        self.streams = [torch.cuda.Stream(device=self.dev) for _ in range(streams)]
+
+    @property
+    def h2d_bytes(self) -> int:
+        return sum(g["c1"] - g["c0"] for g in self.groups)
+
+    @property
+    def d2h_bytes(self) -> int:
+        return sum(g["o1"] - g["o0"] for g in self.groups)
+
+    def run(self, h_comp: torch.Tensor, h_out: torch.Tensor, use_graph: bool = True) -> None:
+        """h_comp/h_out pinned uint8 covering the set's input and output.  Returns after every
+        output is in h_out; raises CodagError with the per-file status if a file failed."""
+        main = torch.cuda.current_stream(self.dev)
+        for s in self.streams:
+            s.wait_stream(main)
+        for k, g in enumerate(self.groups):
+            s = self.streams[k % len(self.streams)]
+            with torch.cuda.stream(s):
+                self.d_comp[g["c0"]:g["c1"]].copy_(h_comp[g["c0"]:g["c1"]], non_blocking=True)
+                g["plan"].run(self.d_comp, self.d_out, self.d_st[g["a"]:g["b"]], use_graph=use_graph, stream=s)
+                h_out[g["o0"]:g["o1"]].copy_(self.d_out[g["o0"]:g["o1"]], non_blocking=True)
+        for s in self.streams:
+            main.wait_stream(s)
+        main.synchronize()
+        _status_error("BatchHostPipeline", self.d_st)
+
+    def close(self) -> None:
+        for g in self.groups:
+            g["plan"].close()
+
+
 @dataclass
 class ChunkSet:
     """Independent compressed chunks packed into one buffer, with their descriptors."""

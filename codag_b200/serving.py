@@ -167,8 +167,21 @@ def poisson_arrivals(rate: float, duration: float, n_files: int, seed: int):
     return list(zip(t.tolist(), rng.integers(0, n_files, t.size).tolist()))
 
 
+def admission_capacity(budget_bytes: int, free_bytes: int, reserve_bytes: int) -> int:
+    """Output bytes the server may hold for admitted requests: the configured budget, but no
+    more than the device memory that is free once the request pool is resident, less a
+    reserve for the per-launch buffers and the verification copies."""
+    return max(0, min(int(budget_bytes), int(free_bytes) - int(reserve_bytes)))
+
+
 class Server:
-    """The request loop on one GPU (see the module docstring)."""
+    """The request loop on one GPU (see the module docstring).
+
+    Requests are admitted by free device memory: the output arena is sized, after the pool
+    is resident, to the smaller of the budget and the device's free memory less a reserve
+    (admission_capacity), and a request waits until the arena grants its output region."""
+
+    RESERVE = 2 << 30  # per-launch descriptor/status buffers and allocator slack
 
     def __init__(self, pool: Pool, budget_bytes: int, slots: int = 4, tune=None, device="cuda",
                  keep_outputs: bool = False, max_chunks_per_launch: int | None = None):
@@ -176,9 +189,13 @@ class Server:
         self.torch = torch
         self.pool = pool
         self.dev = torch.device(device)
-        self.arena = Arena(budget_bytes)
         self.d_comp = torch.from_numpy(pool.comp).to(self.dev)
         self.d_src = torch.from_numpy(pool.src).to(self.dev)
+        free, _ = torch.cuda.mem_get_info(self.dev)
+        self.budget = budget_bytes
+        self.arena = Arena(admission_capacity(budget_bytes, free, self.RESERVE))
+        if self.arena.capacity < CH:
+            raise MemoryError(f"no device memory left for request outputs ({free} bytes free)")
         self.d_out = torch.empty(self.arena.capacity, dtype=torch.uint8, device=self.dev)
         self.tune = native.Tune(*tune, 0) if tune else None
         cap = max_chunks_per_launch or max(1, self.arena.capacity // CH)

@@ -123,3 +123,24 @@ def test_batched_reports_corrupt_file_and_decodes_the_rest(cuda, small_set):
         plan.close()
     s = st.cpu().numpy()
     assert s[bad] == 2 and np.count_nonzero(s) == 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("groups", [1, 3, 7])
+def test_batch_host_pipeline_matches_source(cuda, small_set, groups):
+    """Host-to-host decode of a mixed set with the copies and launches of file groups
+    overlapped on three streams, twice in a row (graphs captured, then replayed)."""
+    from codag_b200 import api
+    ms = small_set
+    h_comp = cuda.from_numpy(ms.comp).pin_memory()
+    h_out = cuda.full((ms.out_bytes,), 0x5A, dtype=cuda.uint8).pin_memory()
+    pipe = api.BatchHostPipeline(ms.descs, ms.comp.size, ms.out_bytes, groups=groups)
+    try:
+        assert len(pipe.groups) == min(groups, ms.n)
+        assert pipe.h2d_bytes <= ms.comp.size and pipe.d2h_bytes <= ms.out_bytes
+        for _ in range(2):
+            h_out.fill_(0x5A)
+            pipe.run(h_comp, h_out)
+            assert np.array_equal(h_out.numpy(), ms.expected())
+    finally:
+        pipe.close()

@@ -91,3 +91,22 @@ def test_mixed_requests_equal_alone(cuda, small_pool):
         assert np.array_equal(got, p.src[f.src_off:f.src_off + f.size])
     s = serving.summarize(reqs, p, 0.03)
     assert s["bit_exact"] and s["completed"] == 60 and s["p99_ms"] >= s["p50_ms"] > 0
+
+
+def test_admission_capacity_follows_free_memory():
+    GiB = 1 << 30
+    assert serving.admission_capacity(64 * GiB, 170 * GiB, 2 * GiB) == 64 * GiB  # the budget binds
+    assert serving.admission_capacity(64 * GiB, 40 * GiB, 2 * GiB) == 38 * GiB   # free memory binds
+    assert serving.admission_capacity(64 * GiB, 1 * GiB, 2 * GiB) == 0
+
+
+@pytest.mark.gpu
+def test_server_admits_by_free_device_memory(cuda, small_pool):
+    """A budget far above the device's memory is cut to what is free: requests are still
+    admitted and decoded, bit-exact."""
+    free, _ = cuda.cuda.mem_get_info()
+    pool = small_pool
+    srv = serving.Server(pool, 1 << 50, slots=2)
+    assert srv.arena.capacity <= free - serving.Server.RESERVE
+    reqs = srv.run(serving.poisson_arrivals(400, 0.05, len(pool.files), 3))
+    assert reqs and all(r.ok for r in reqs)
