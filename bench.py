@@ -336,6 +336,38 @@ def measure_codec(workload: str, args, rank: int, world: int, local: int, steps:
     }
 
 
+def measure_encode(workload: str, local: int, steps: int = 5) -> dict:
+    """GPU encoder (codag_compress_rlev1/_rlev2) on a per-codec column resident in HBM: input
+    GB/s, and whether the file equals the host producer's byte for byte."""
+    import torch
+    from codag_b200 import api, native as nat
+    w = WORKLOADS[workload]
+    codec, e = w["codec"], w["elem"]
+    f = make_file(workload, 0)
+    dev = torch.device("cuda", local)
+    d_col = torch.from_numpy(f["col"]).to(dev)
+    need = int(nat.lib().codag_compress_workspace_bytes(codec, d_col.numel(), CH, e))
+    ws = torch.empty(need + 256, dtype=torch.uint8, device=dev)
+    out = api.compress_rle(codec, d_col, CH, e, ws=ws)  # warm-up
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(steps):
+        out = api.compress_rle(codec, d_col, CH, e, ws=ws)
+    t1.record()
+    torch.cuda.synchronize()
+    dt = t0.elapsed_time(t1) / 1e3 / steps
+    blob = out[0].cpu().numpy()
+    want = np.concatenate([np.frombuffer(np.uint64(f["col"].size).tobytes(), np.uint8), f["comp"]]) if codec == 0 \
+        else f["comp"]
+    ok = bool(np.array_equal(blob, want))
+    del d_col, ws, out
+    torch.cuda.empty_cache()
+    return {"workload": "GPU encode of " + w["desc"], "value": round(f["col"].size / dt / 1e9, 2), "unit": "GB/s",
+            "ms_per_step": round(dt * 1e3, 3), "bit_exact_vs_host_producer": ok,
+            "how": "codag_compress_rlev1/_rlev2: one thread per chunk, scan, gather; input bytes per second"}
+
+
 def _summary(line: dict) -> dict:
     """The figures of a per-codec line kept under the headline's `configs`."""
     keep = ("value", "unit", "ms_per_step", "bit_exact", "e2e", "roofline", "cpu_baseline", "clocks")
@@ -400,6 +432,8 @@ def main():
                 for wl in EXTRA_CONFIGS:
                     configs[wl] = _summary(measure_codec(wl, args, rank, world, local, args.extra_steps, 3,
                                                          clocks_on=False))
+                configs["encode_rlev2"] = measure_encode("rlev2", local)
+                configs["encode_rlev1"] = measure_encode("rlev1x128", local)
                 configs["serving"] = bench_serving.short_sweep(args, local)
                 line["configs"] = configs
                 line["configs_note"] = ("per-codec configurations and a short serving sweep, timed in the same run "

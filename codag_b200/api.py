@@ -99,6 +99,34 @@ def decompress_deflate(comp: torch.Tensor, blk_off: torch.Tensor, chunk_bytes: i
         out.numel() if out_bytes is None else out_bytes, _dptr(status), _stream(stream)))
 
 
+def compress_rle(codec: int, col: torch.Tensor, chunk_bytes: int = 131072, elem_bytes: int = 8, stream=None,
+                 ws: torch.Tensor | None = None):
+    """GPU encoder (codag_compress_rlev1/_rlev2) of a device column (uint8 view): returns
+    (file, blk_off, col_len) as device tensors in CODAG's layout, the same bytes as
+    native.encode_rlev1/encode_rlev2 write on the host (the RLE v1 file is the blob
+    [u64 size][streams]).  The output buffers (and the workspace unless given) are allocated
+    here; the C ABI itself allocates nothing."""
+    lib = native.lib()
+    n_bytes = col.numel()
+    n = int(lib.codag_compress_chunks(n_bytes, chunk_bytes))
+    cap = int(lib.codag_compress_bound(codec, n_bytes, chunk_bytes, elem_bytes))
+    need = int(lib.codag_compress_workspace_bytes(codec, n_bytes, chunk_bytes, elem_bytes))
+    dev = col.device
+    if ws is None or ws.numel() < need:
+        ws = torch.empty(need + 256, dtype=torch.uint8, device=dev)
+    wsp = (ws.data_ptr() + 255) // 256 * 256
+    out = torch.empty(cap, dtype=torch.uint8, device=dev)
+    blk_off = torch.empty(n + 1, dtype=torch.int64, device=dev)
+    col_len = torch.empty(n, dtype=torch.int64, device=dev)
+    meta = torch.zeros(2, dtype=torch.int64, device=dev)  # [file bytes, status]
+    fn = lib.codag_compress_rlev1 if codec == native.RLEV1 else lib.codag_compress_rlev2
+    check("codag_compress", fn(_dptr(col), n_bytes, chunk_bytes, elem_bytes, _dptr(out), cap, _dptr(blk_off),
+                               _dptr(col_len), _dptr(meta), _dptr(meta) + 8, wsp, need, _stream(stream)))
+    nbytes, status = (int(x) for x in meta.cpu())
+    check("codag_compress (device status)", status & 0xffffffff)
+    return out[:nbytes], blk_off, col_len
+
+
 def selftest_wait_timeout(wait_cycles: int = 2_000_000) -> int:
     """Runs the bounded-wait self test and returns the status it reports (expect ETIMEOUT)."""
     native.set_wait_limit(wait_cycles)
@@ -158,6 +186,22 @@ def decompress_deflate_host(comp: np.ndarray, blk_offset: np.ndarray, chunk_byte
     st = torch.zeros(n, dtype=torch.int32, device="cuda")
     decompress_deflate(d_comp, d_off, chunk_bytes, out, wrapper_bytes, size, st)
     _status_error("deflate", st)
+    return out.cpu().numpy()
+
+
+def decompress_cudf_deflate_host(file: np.ndarray) -> np.ndarray:
+    """A file in CODAG's cuDF-comparison layout (rapids_compressor.py:222-275) in, the n chunks
+    decoded out (n x chunk size bytes, as CODAG's base_deflate tool writes them,
+    include/base_deflate.h:20-130): the layout is parsed on the host and the streams go to
+    codag_decompress_deflate."""
+    chunk, data, rel = native.cudf_deflate_layout(file)
+    n = rel.size - 1
+    d_comp = _h2d(np.ascontiguousarray(file[data:]))
+    d_off = _h2d(rel.view(np.int64))
+    out = torch.empty(n * chunk, dtype=torch.uint8, device="cuda")
+    st = torch.zeros(n, dtype=torch.int32, device="cuda")
+    decompress_deflate(d_comp, d_off, chunk, out, 2, n * chunk, st)
+    _status_error("cudf deflate", st)
     return out.cpu().numpy()
 
 
@@ -288,8 +332,9 @@ class BatchHostPipeline:
     group's decode and a third group's device-to-host copy overlap, and the launches of
     different groups overlap on the GPU as well (a launch ends with its longest file while the
     next one fills the other SMs).  Files must be packed in index order, as pack_chunks and
-    codag_encode_set do, so each group's input and output are contiguous ranges.  Device
-    buffers and plans live as long as the pipeline; bytes between outputs are zero."""
+    codag_encode_set do, so each group's input and output are contiguous ranges; the output
+    ranges tile the whole output buffer.  Device buffers and plans live as long as the
+    pipeline; bytes between and after the files' outputs come back as zeros."""
 
     def __init__(self, descs: np.ndarray, comp_bytes: int, out_bytes: int, groups: int = 6, streams: int = 3,
                  shape: tuple | None = None, device="cuda"):
@@ -308,6 +353,11 @@ class BatchHostPipeline:
                 a=int(a), b=int(b), plan=BatchPlan(d, *(shape or ())),
                 c0=int(d["comp_off"].min()), c1=int((d["comp_off"] + d["comp_len"]).max()),
                 o0=int(d["out_off"].min()), o1=int((d["out_off"] + d["out_len"]).max())))
+        # output ranges tile [0, out_bytes): the bytes between and after files come back as zeros
+        for k, g in enumerate(self.groups):
+            g["o0"] = 0 if k == 0 else self.groups[k - 1]["o1"]
+            if k == len(self.groups) - 1:
+                g["o1"] = max(out_bytes, g["o1"])
         self.d_comp = torch.empty(max(comp_bytes, 1), dtype=torch.uint8, device=self.dev)
         self.d_out = torch.zeros(max(out_bytes, 1), dtype=torch.uint8, device=self.dev)
         self.d_st = torch.zeros(max(n, 1), dtype=torch.int32, device=self.dev)

@@ -3,7 +3,8 @@
 Produces, next to the sources:
   codag_b200/libcodag_b200.so   CUDA decoders (sm_100a) and the C ABI of include/codag.h
   codag_b200/libcodag_fmt.so    host-only format producers and generators (include/codag_format.h)
-  build/exe/src/<codec>/<codec>.cu.exe   CLIs with CODAG's command lines (rlev1, rlev2, zlib)
+  build/exe/src/<dir>/<tool>.cu.exe   CLIs with CODAG's command lines (rlev1, rlev2, zlib,
+                                      util/base_deflate)
 
 Run ``python -m codag_b200.build`` (or ``__graft_entry__.build()``).  nvcc cross-compiles
 for sm_100a without a GPU.
@@ -29,11 +30,13 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fop
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fopenmp", "-Wall", "-Wno-unused-function"]
 
 HOST_SOURCES = sorted((CSRC / "host").glob("*.cpp"))
-CUDA_SOURCES = [CSRC / "kernels" / "codag_capi.cu"]
+CUDA_SOURCES = [CSRC / "kernels" / "codag_capi.cu", CSRC / "kernels" / "encode_capi.cu"]
 CUDA = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 HEADERS = (sorted(CSRC.rglob("*.cuh")) + sorted(CSRC.rglob("*.hpp")) + sorted(CSRC.glob("*.h")) +
            [REPO / "include" / "codag.h", REPO / "include" / "codag_format.h"])
-CLI_SOURCES = {name: CSRC / "cli" / f"{name}_main.cpp" for name in ("rlev1", "rlev2", "zlib")}
+CLI_SOURCES = {name: CSRC / "cli" / f"{name}_main.cpp" for name in ("rlev1", "rlev2", "zlib", "base_deflate")}
+# where CODAG's Makefile puts each tool (build/exe/src/<dir>/<name>.cu.exe)
+CLI_DIRS = {"rlev1": "rlev1", "rlev2": "rlev2", "zlib": "zlib", "base_deflate": "util"}
 
 
 def _run(cmd: list[str], verbose: bool) -> None:
@@ -76,7 +79,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     for name, src in CLI_SOURCES.items():
         if not src.exists():
             continue
-        exe = EXE / name / f"{name}.cu.exe"
+        exe = EXE / CLI_DIRS[name] / f"{name}.cu.exe"
         exe.parent.mkdir(parents=True, exist_ok=True)
         if force or _stale(exe, [src, LIB, FMT_LIB, CSRC / "cli" / "cli_common.hpp"] + HEADERS):
             _run(["g++", "-O2", "-std=c++17", "-Wall", src, "-I", REPO / "include", "-I", CUDA / "include", "-o", exe,

@@ -142,6 +142,59 @@ extern "C" codag_status codag_encode_deflate(const uint8_t* in, uint64_t in_byte
   return CODAG_OK;
 }
 
+// The layout CODAG's cuDF comparison reads (rapids_compressor.py:222-275 writes it,
+// include/base_deflate.h:20-130 decodes it): [u64 chunk_bytes][u64 n][u64 size_i x n] followed
+// by the n zlib streams back to back, no padding; chunk i holds bytes [i*chunk, (i+1)*chunk)
+// of the input zero padded to a multiple of chunk_bytes.
+extern "C" codag_status codag_encode_cudf_deflate(const uint8_t* in, uint64_t in_bytes, uint64_t chunk_bytes, int level,
+                                                  codag_hbuf* file) {
+  if (!in || !file || chunk_bytes == 0 || in_bytes == 0 || level < 0 || level > 9) return CODAG_EINVAL;
+  const uint64_t n = (in_bytes + chunk_bytes - 1) / chunk_bytes;
+  std::vector<uint8_t> padded(n * chunk_bytes, 0);
+  std::memcpy(padded.data(), in, in_bytes);
+  std::vector<std::vector<uint8_t>> streams;
+  if (encode_chunks(padded, n, chunk_bytes, streams, [&](const uint8_t* c, uint64_t b, std::vector<uint8_t>& o) {
+        return deflate_encode_chunk(c, b, level, 1, Z_DEFAULT_STRATEGY, o, nullptr);
+      }))
+    return CODAG_EINVAL;
+  uint64_t total = 16 + 8 * n;
+  for (const auto& st : streams) total += st.size();
+  std::vector<uint8_t> out(total);
+  uint64_t* head = reinterpret_cast<uint64_t*>(out.data());
+  head[0] = chunk_bytes;
+  head[1] = n;
+  uint64_t pos = 16 + 8 * n;
+  for (uint64_t i = 0; i < n; i++) {
+    head[2 + i] = streams[i].size();
+    std::memcpy(out.data() + pos, streams[i].data(), streams[i].size());
+    pos += streams[i].size();
+  }
+  return to_hbuf(out.data(), out.size(), file) ? CODAG_OK : CODAG_ENOMEM;
+}
+
+extern "C" codag_status codag_cudf_deflate_layout(const uint8_t* file, uint64_t file_bytes, uint64_t* chunk_bytes,
+                                                  uint64_t* n_chunks, uint64_t* data_offset, uint64_t* blk_off) {
+  if (!file || !chunk_bytes || !n_chunks || !data_offset || file_bytes < 16) return CODAG_EINVAL;
+  uint64_t head[2];
+  std::memcpy(head, file, 16);
+  const uint64_t n = head[1];
+  if (head[0] == 0 || head[0] >= (1ull << 31) || n > (file_bytes - 16) / 8) return CODAG_EINVAL;
+  const uint64_t data = 16 + 8 * n;
+  uint64_t cum = 0;
+  for (uint64_t i = 0; i < n; i++) {
+    uint64_t sz;
+    std::memcpy(&sz, file + 16 + 8 * i, 8);
+    if (sz > file_bytes - data - cum) return CODAG_EINVAL;  // stream i must lie inside the file
+    if (blk_off) blk_off[i] = cum;
+    cum += sz;
+  }
+  if (blk_off) blk_off[n] = cum;
+  *chunk_bytes = head[0];
+  *n_chunks = n;
+  *data_offset = data;
+  return CODAG_OK;
+}
+
 extern "C" codag_status codag_encode_one(int codec, const uint8_t* in, uint64_t in_bytes, int elem_bytes,
                                          int level, codag_hbuf* stream) {
   if (!in || !stream || in_bytes == 0) return CODAG_EINVAL;

@@ -1,408 +1,14 @@
-// ORC RLE v2 chunk encoder (host, unsigned values).  Produces the byte stream of CODAG's
-// encoder include/rlev2/encoder_trans.h:184-357 (block_encode_orig) with the helpers of
-// include/rlev2/encoder.h:56-591 (determineEncoding, the four header writers, the patch-list
-// builder and the bit/percentile helpers), so our files and CODAG's are interchangeable.
-//
-// One thread of CODAG's encoder walks one chunk.  It keeps up to 128 pending values, tracks
-// a fixed run (equal values) and a variable run, and when a run is closed chooses among
-//   SHORT_REPEAT  3..10 equal values, value in 1..8 big-endian bytes
-//   DELTA         fixed step (width code 0) or monotonic packed deltas
-//   DIRECT        values bit packed at an aligned width
-//   PATCHED_BASE  base-reduced values at the 95th-percentile width plus (gap, patch) pairs
-// Values are zero-extended to 64 bits and are never zigzagged (include/rlev2/utils.h:8);
-// only the DELTA base delta is a signed varint.  Deliberately kept behaviours of the
-// reference encoder: runs are cut at 128 values; a pending group with minimum 0 and maximum
-// <= 128 is written DIRECT (is_safe_subtract, encoder.h:55-60); the width of DELTA deltas is
-// computed on the unsigned deltas.
-#include <algorithm>
+// ORC RLE v2 chunk encoder (host, unsigned values): the shared writer of ../rle_writers.h over
+// a growing byte vector.  The layout (include/rlev2/encoder_trans.h:482-564) is written by
+// capi_host.cpp.
 #include <cstdint>
 #include <cstring>
 #include <vector>
 
-#include "../rlev2_widths.h"
+#include "../rle_writers.h"
 #include "host_common.hpp"
 
 namespace codag_host {
-namespace {
-
-constexpr int kMaxLiterals = 128;  // utils.h:64
-constexpr int kMinRepeat = 3;      // utils.h:65
-constexpr int kMaxShortRepeat = 10;
-
-// number of significant bits rounded up to a representable width (find_closes_num_bits)
-inline uint8_t closest_width(uint64_t v) {
-  uint8_t c = 0;
-  while (v) {
-    v >>= 1;
-    ++c;
-  }
-  return v2_closest(c);
-}
-
-class RleV2Writer {
- public:
-  explicit RleV2Writer(std::vector<uint8_t>& out) : out_(out) { std::fill(deltas_, deltas_ + kMaxLiterals, 0); }
-
-  void encode(const uint64_t* v, uint64_t n) {
-    uint64_t prev_delta = 0;
-    for (uint64_t i = 0; i < n; i++) {
-      const uint64_t val = v[i];
-      if (nlit_ == 0) {
-        lit_[nlit_++] = val;
-        fix_ = 1;
-        var_ = 1;
-        continue;
-      }
-      if (nlit_ == 1) {
-        lit_[nlit_++] = val;
-        prev_delta = val - lit_[0];
-        if (val == lit_[0]) {
-          fix_ = 2;
-          var_ = 0;
-        } else {
-          fix_ = 0;
-          var_ = 2;
-        }
-        continue;
-      }
-      const uint64_t cur_delta = val - lit_[nlit_ - 1];
-      if (prev_delta == 0 && cur_delta == 0) {
-        lit_[nlit_++] = val;
-        if (var_ > 0) fix_ = 2;  // the fixed run is the tail of the pending values
-        fix_++;
-        if (fix_ >= kMinRepeat && var_ > 0) {
-          nlit_ -= kMinRepeat;
-          var_ -= kMinRepeat - 1;
-          choose_encoding();
-          prev_delta = 0;
-          for (int k = 0; k < kMinRepeat; ++k) {
-            lit_[k] = val;
-            deltas_[k] = 0;
-          }
-          nlit_ = kMinRepeat;
-        } else if (fix_ >= kMinRepeat) {
-          deltas_[0] = 0;
-        }
-        if (fix_ == kMaxLiterals) choose_encoding();
-        continue;
-      }
-      if (fix_ >= kMinRepeat) {
-        if (fix_ <= kMaxShortRepeat) {
-          write_short_repeat();
-        } else {
-          fixed_delta_ = true;
-          write_delta();
-        }
-      }
-      if (fix_ > 0 && fix_ < kMinRepeat && val != lit_[nlit_ - 1]) {
-        var_ = fix_;
-        fix_ = 0;
-      }
-      if (nlit_ == 0) {
-        lit_[nlit_++] = val;
-        fix_ = 1;
-        var_ = 1;
-      } else {
-        prev_delta = val - lit_[nlit_ - 1];
-        lit_[nlit_++] = val;
-        var_++;
-        if (var_ == kMaxLiterals) choose_encoding();
-      }
-    }
-    if (nlit_ != 0) {
-      if (var_ != 0) {
-        choose_encoding();
-      } else if (fix_ != 0) {
-        if (fix_ < kMinRepeat) {
-          var_ = fix_;
-          fix_ = 0;
-          choose_encoding();
-        } else if (fix_ <= kMaxShortRepeat) {
-          write_short_repeat();
-        } else {
-          fixed_delta_ = true;
-          write_delta();
-        }
-      }
-    }
-  }
-
- private:
-  void put(uint8_t b) { out_.push_back(b); }
-
-  // histogram of representable widths (compute_bit_width)
-  static void width_hist(const uint64_t* d, uint32_t n, uint8_t* hist) {
-    std::fill(hist, hist + 32, 0);
-    for (uint32_t i = 0; i < n; ++i) hist[v2_code(closest_width(d[i]))]++;
-  }
-
-  // smallest width covering all but the top (100-p)% of values (compute_percentile_bit_width)
-  static uint8_t percentile_width(const uint8_t* hist, uint32_t n, uint8_t p) {
-    p = std::min<uint8_t>(static_cast<uint8_t>(100 - p), 100);
-    int32_t left = (p == 0 ? 0 : static_cast<int32_t>((n * p - 1) / 100 + 1));
-    for (int8_t i = 31; i >= 0; --i) {
-      left -= hist[i];
-      if (left < 0) return v2_width(i);
-    }
-    return 0;
-  }
-
-  // fixed width big-endian packing used by DIRECT and DELTA (write_aligned_ints)
-  void put_aligned(const uint64_t* d, uint32_t n, uint8_t bits) {
-    if (bits < 8) {
-      const uint8_t mask = static_cast<uint8_t>((1 << bits) - 1);
-      const uint32_t per_byte = 8 / bits;
-      const uint32_t rem = n % per_byte;
-      const uint32_t full = n - rem;
-      for (uint32_t i = 0; i < full; i += per_byte) {
-        uint8_t b = 0;
-        for (uint32_t j = 0; j < per_byte; ++j)
-          b |= static_cast<uint8_t>((d[i + j] & mask) << (8 - (j + 1) * bits));
-        put(b);
-      }
-      if (rem > 0) {
-        uint32_t shift = 8 - bits;
-        uint8_t b = 0;
-        for (uint32_t i = full; i < n; ++i) {
-          b |= static_cast<uint8_t>((d[i] & mask) << shift);
-          shift -= bits;
-        }
-        put(b);
-      }
-    } else {
-      const int bytes = bits / 8;
-      for (uint32_t i = 0; i < n; ++i)
-        for (int j = bytes - 1; j >= 0; --j) put(static_cast<uint8_t>((d[i] >> (j * 8)) & 0xff));
-    }
-  }
-
-  // MSB-first packing at any width (write_unaligned_ints)
-  void put_unaligned(const uint64_t* d, uint32_t n, uint8_t bits) {
-    uint32_t room = 8;
-    uint8_t cur = 0;
-    for (uint32_t i = 0; i < n; ++i) {
-      uint64_t value = d[i];
-      uint32_t todo = bits;
-      while (todo > room) {
-        cur |= static_cast<uint8_t>(value >> (todo - room));
-        todo -= room;
-        value &= (static_cast<uint64_t>(1) << todo) - 1;
-        put(cur);
-        cur = 0;
-        room = 8;
-      }
-      room -= todo;
-      cur |= static_cast<uint8_t>(value << room);
-      if (room == 0) {
-        put(cur);
-        cur = 0;
-        room = 8;
-      }
-    }
-    if (room != 8) put(cur);
-  }
-
-  void put_uvarint(int64_t val) {
-    for (;;) {
-      if ((val & ~0x7f) == 0) {
-        put(static_cast<uint8_t>(val));
-        return;
-      }
-      put(static_cast<uint8_t>(0x80 | (val & 0x7f)));
-      val = static_cast<int64_t>(static_cast<uint64_t>(val) >> 7);
-    }
-  }
-  void put_svarint(int64_t val) { put_uvarint((val << 1) ^ (val >> 63)); }
-
-  void write_short_repeat() {
-    const uint64_t val = lit_[0];
-    const uint8_t nbytes = static_cast<uint8_t>((closest_width(val) - 1) / 8 + 1);
-    put(static_cast<uint8_t>(((nbytes - 1) << 3) | (fix_ - kMinRepeat)));
-    for (int i = nbytes - 1; i >= 0; i--) put(static_cast<uint8_t>((val >> (i * 8)) & 0xff));
-    fix_ = 0;
-    nlit_ = 0;
-    var_ = 0;
-  }
-
-  void write_direct() {
-    uint8_t hist[32];
-    width_hist(lit_, nlit_, hist);
-    const uint8_t bits = v2_closest_aligned(percentile_width(hist, nlit_, 100));
-    const uint16_t enc = v2_code(bits);
-    // The reference writes var_runlen-1 here.  On every path var_runlen equals the number
-    // of pending values except one: a 128-value run of zeros reaches this writer through
-    // is_safe_subtract with var_runlen == 0, and the reference emits a length field of 511
-    // over 128 packed values, a stream no decoder reads back.  Counting the pending values
-    // gives the same bytes everywhere else and a decodable header there.
-    const uint16_t len = static_cast<uint16_t>(nlit_ - 1);
-    put(static_cast<uint8_t>(0x40 | (enc << 1) | ((len & 0x100) >> 8)));
-    put(static_cast<uint8_t>(len & 0xff));
-    put_aligned(lit_, nlit_, bits);
-    var_ = 0;
-    nlit_ = 0;
-  }
-
-  void write_delta() {
-    uint16_t len;
-    uint8_t enc = 0;
-    uint8_t bits = v2_closest_aligned(delta_bits_);
-    if (fixed_delta_) {
-      if (fix_ > kMinRepeat) {
-        len = static_cast<uint16_t>(fix_ - 1);
-        fix_ = 0;
-      } else {
-        len = static_cast<uint16_t>(var_ - 1);
-        var_ = 0;
-      }
-    } else {
-      if (bits == 1) bits = 2;
-      enc = v2_code(bits);
-      len = static_cast<uint16_t>(var_ - 1);
-      var_ = 0;
-    }
-    put(static_cast<uint8_t>(0xC0 | (enc << 1) | ((len & 0x100) >> 8)));
-    put(static_cast<uint8_t>(len & 0xff));
-    put_uvarint(static_cast<int64_t>(lit_[0]));
-    put_svarint(static_cast<int64_t>(deltas_[0]));
-    if (!fixed_delta_) put_aligned(deltas_ + 1, nlit_ - 2, bits);
-    for (uint32_t i = 0; i < nlit_; ++i) deltas_[i] = 0;
-    nlit_ = 0;
-    var_ = 0;
-  }
-
-  void write_patched(uint64_t lit_min, uint8_t b95, uint8_t b100, uint64_t* reduced) {
-    // patch list (preparePatchedBlob1, encoder.h:182-268)
-    int64_t mask = static_cast<int64_t>((static_cast<uint64_t>(1) << b95) - 1);
-    uint32_t pwidth = v2_closest(b100 - b95);
-    if (pwidth == 64) {
-      pwidth = 56;
-      b95 = 8;
-      mask = static_cast<int64_t>((static_cast<uint64_t>(1) << b95) - 1);
-    }
-    uint64_t gaps[kMaxLiterals], patches[kMaxLiterals], list[kMaxLiterals];
-    uint32_t npatch = 0;
-    size_t prev = 0, max_gap = 0;
-    for (size_t i = 0; i < nlit_; i++) {
-      if (reduced[i] > static_cast<uint64_t>(mask)) {
-        size_t gap = i - prev;
-        if (gap > max_gap) max_gap = gap;
-        prev = i;
-        gaps[npatch] = gap;
-        patches[npatch] = reduced[i] >> b95;
-        npatch++;
-        reduced[i] &= static_cast<uint64_t>(mask);
-      }
-    }
-    uint32_t gap_width;
-    if (max_gap == 0 && npatch != 0)
-      gap_width = 1;
-    else
-      gap_width = closest_width(max_gap);
-    uint32_t nlist = npatch;
-    if (gap_width > 8) {  // unreachable with 128-value groups; kept for format fidelity
-      gap_width = 8;
-      nlist += (max_gap == 511) ? 2 : 1;
-    }
-    uint32_t pos = 0;
-    for (uint32_t i = 0, gi = 0; i < nlist; i++) {
-      uint64_t g = gaps[gi], p = patches[gi];
-      gi++;
-      while (g > 255) {
-        list[pos++] = 255ull << pwidth;
-        i++;
-        g -= 255;
-      }
-      list[pos++] = (g << pwidth) | p;
-    }
-
-    // header and body (writePatchedBasedValues, encoder.h:527-591)
-    uint32_t len = var_ - 1;
-    const uint8_t h0 = static_cast<uint8_t>(0x80 | (v2_code(b95) << 1) | ((len & 0x100) >> 8));
-    const uint8_t h1 = static_cast<uint8_t>(len & 0xff);
-    const uint32_t base_bits = closest_width(lit_min) + 1;
-    const uint32_t base_bytes = (base_bits - 1) / 8 + 1;
-    const uint8_t h2 = static_cast<uint8_t>(((base_bytes - 1) << 5) | v2_code(pwidth));
-    const uint8_t h3 = static_cast<uint8_t>((gap_width - 1) << 5 | nlist);
-    put(h0);
-    put(h1);
-    put(h2);
-    put(h3);
-    for (int i = static_cast<int>(base_bytes) - 1; i >= 0; i--) put(static_cast<uint8_t>((lit_min >> (i * 8)) & 0xff));
-    put_unaligned(reduced, nlit_, v2_closest(b95));
-    put_unaligned(list, nlist, v2_closest(gap_width + pwidth));
-    var_ = 0;
-    nlit_ = 0;
-  }
-
-  // determineEncoding (encoder.h:270-387)
-  void choose_encoding() {
-    if (nlit_ <= static_cast<uint32_t>(kMinRepeat)) {
-      write_direct();
-      return;
-    }
-    bool increasing = true, decreasing = true;
-    fixed_delta_ = true;
-    uint64_t lmin = lit_[0], lmax = lit_[0];
-    const uint64_t initial = lit_[1] - lit_[0];
-    uint64_t max_delta = 0;
-    for (uint32_t i = 1; i < nlit_; i++) {
-      const uint64_t l1 = lit_[i], l0 = lit_[i - 1];
-      const uint64_t d = l1 - l0;
-      lmin = std::min(lmin, l1);
-      lmax = std::max(lmax, l1);
-      increasing &= (l0 <= l1);
-      decreasing &= (l0 >= l1);
-      fixed_delta_ &= (d == initial);
-      deltas_[i - 1] = d;
-      max_delta = std::max(max_delta, d);
-    }
-    deltas_[0] = lit_[1] - lit_[0];
-    // is_safe_subtract on unsigned values: only a minimum of 0 with maximum <= 128 fails
-    const bool safe = (lmin > 0) || (lmax > static_cast<uint64_t>(lmin - INT8_MIN));
-    if (!safe) {
-      write_direct();
-      return;
-    }
-    if (lmin == lmax || fixed_delta_) {
-      write_delta();
-      return;
-    }
-    if (initial != 0) {
-      delta_bits_ = closest_width(max_delta);
-      if (increasing || decreasing) {
-        write_delta();
-        return;
-      }
-    }
-    uint8_t hist[32];
-    width_hist(lit_, nlit_, hist);
-    const uint8_t b100 = percentile_width(hist, nlit_, 100);
-    const uint8_t b90 = percentile_width(hist, nlit_, 90);
-    if (static_cast<uint32_t>(b100 - b90) > 1) {
-      uint64_t reduced[kMaxLiterals];
-      for (uint32_t i = 0; i < nlit_; i++) reduced[i] = lit_[i] - lmin;
-      width_hist(reduced, nlit_, hist);
-      const uint8_t r95 = percentile_width(hist, nlit_, 95);
-      const uint8_t r100 = percentile_width(hist, nlit_, 100);
-      if (r100 - r95 != 0) {
-        write_patched(lmin, r95, r100, reduced);
-      } else {
-        write_direct();
-      }
-      return;
-    }
-    write_direct();
-  }
-
-  std::vector<uint8_t>& out_;
-  uint64_t lit_[kMaxLiterals] = {};
-  uint64_t deltas_[kMaxLiterals];
-  uint32_t nlit_ = 0, fix_ = 0, var_ = 0;
-  uint8_t delta_bits_ = 0;
-  bool fixed_delta_ = false;
-};
-
-}  // namespace
 
 int rlev2_encode_chunk(const uint8_t* chunk, uint64_t chunk_bytes, int elem_bytes,
                        std::vector<uint8_t>& out) {
@@ -410,14 +16,13 @@ int rlev2_encode_chunk(const uint8_t* chunk, uint64_t chunk_bytes, int elem_byte
       chunk_bytes % elem_bytes)
     return CODAG_EINVAL;
   const uint64_t n = chunk_bytes / elem_bytes;
-  std::vector<uint64_t> vals(n);
-  for (uint64_t i = 0; i < n; i++) {
+  VectorSink sink{out};
+  codag_fmt::RleV2Writer<VectorSink> w(sink);
+  w.encode([&](uint64_t i) {
     uint64_t v = 0;
     std::memcpy(&v, chunk + i * elem_bytes, elem_bytes);  // little-endian zero extension
-    vals[i] = v;
-  }
-  RleV2Writer w(out);
-  w.encode(vals.data(), n);
+    return v;
+  }, n);
   return CODAG_OK;
 }
 

@@ -8,6 +8,14 @@
 
 namespace codag_host {
 
+// byte sink of the shared RLE writers (../rle_writers.h) over a growing vector
+struct VectorSink {
+  std::vector<uint8_t>& v;
+  void put(uint8_t b) { v.push_back(b); }
+  uint64_t size() const { return v.size(); }
+  void set(uint64_t i, uint8_t b) { v[i] = b; }
+};
+
 // --- per-chunk encoders -------------------------------------------------------------
 // Each appends one compressed stream for `chunk_bytes` bytes of input to `out`.
 int rlev1_encode_chunk(const uint8_t* chunk, uint64_t chunk_bytes, int elem_bytes,

@@ -144,9 +144,9 @@ __device__ __forceinline__ void body_fill(OUT& out, uint32_t n, uint32_t cnt, ui
 template <int NSLOT, int E, class OUT>
 __device__ __forceinline__ void body_unpack(const InRing<NSLOT>& in, OUT& out, uint32_t n, uint32_t cnt, uint32_t bit0,
                                             uint32_t fbw, uint64_t add, uint32_t lane) {
-  if (lane >= cnt) return;
   constexpr uint32_t IM = InRing<NSLOT>::kMask;
   const uint32_t ib = in.sbuf;
+  if (lane >= cnt) return;
   uint32_t bp = bit0 + lane * fbw;
   const uint32_t bstep = fbw << 5;
   uint32_t oa = (n + lane) * E;
@@ -313,41 +313,48 @@ __device__ __forceinline__ int body_literals(InRing<NSLOT>& in, OUT& out, uint32
 // ---------------------------------------------------------------------------------------
 // single-pass decoders: the warp walks the headers itself
 // ---------------------------------------------------------------------------------------
+// RLE v1, one header at pos (all lanes on the same data): expands it and advances pos and n.
+template <int NSLOT, int E, class OUT>
+__device__ __forceinline__ int rlev1_header(InRing<NSLOT>& in, OUT& out, uint32_t& pos, uint32_t& n, uint32_t cap,
+                                            uint32_t end, uint32_t lane) {
+  int st = in.advance(pos, min(pos + 32, end));
+  if (st) return st;
+  const int h = static_cast<int8_t>(in.rd8(pos));
+  uint32_t cnt;
+  if (h >= 0) {  // run: count h+3, int8 delta, varint base (decoder.h:731-790)
+    if (pos + 2 >= end) return CODAG_ECORRUPT;
+    const int64_t delta = static_cast<int8_t>(in.rd8(pos + 1));
+    uint32_t len;
+    uint64_t base;
+    if (!read_uvarint(in, pos + 2, end, len, base)) return CODAG_ECORRUPT;
+    cnt = static_cast<uint32_t>(h) + 3u;
+    if (n + cnt > cap) return CODAG_ECORRUPT;
+    body_fill<E>(out, n, cnt, base, static_cast<uint64_t>(delta), lane);
+    pos += 2 + len;
+  } else {
+    cnt = static_cast<uint32_t>(-h);
+    if (n + cnt > cap) return CODAG_ECORRUPT;
+    pos += 1;
+    st = body_literals<NSLOT, E>(in, out, n, cnt, pos, end, lane);
+    if (st) return st;
+  }
+  n += cnt;
+  __syncwarp();
+  out.flush_to(n * E);
+  return CODAG_OK;
+}
+
 // RLE v1: loops while fewer than cap elements were produced, as the reference does
-// (decoder.h:669).
+// (decoder.h:669); the warp parses one header at a time.
 template <int NSLOT, int E, class OUT>
 __device__ int decode_rlev1_chunk(InRing<NSLOT>& in, OUT& out, uint32_t cap) {
-  const uint32_t lane = in.lane;
-  const uint32_t end = in.hi;
-  uint32_t pos = in.lo;
-  uint32_t n = 0;
+  const uint32_t lane = in.lane, end = in.hi;
+  uint32_t pos = in.lo, n = 0;
   int st = CODAG_OK;
   while (n < cap) {
     if (pos >= end) { st = CODAG_ECORRUPT; break; }
-    st = in.advance(pos, min(pos + 32, end));
+    st = rlev1_header<NSLOT, E>(in, out, pos, n, cap, end, lane);
     if (st) break;
-    const int h = static_cast<int8_t>(in.rd8(pos));
-    uint32_t cnt;
-    if (h >= 0) {  // run: count h+3, int8 delta, varint base (decoder.h:731-790)
-      if (pos + 2 >= end) { st = CODAG_ECORRUPT; break; }
-      const int64_t delta = static_cast<int8_t>(in.rd8(pos + 1));
-      uint32_t len;
-      uint64_t base;
-      if (!read_uvarint(in, pos + 2, end, len, base)) { st = CODAG_ECORRUPT; break; }
-      cnt = static_cast<uint32_t>(h) + 3u;
-      if (n + cnt > cap) { st = CODAG_ECORRUPT; break; }
-      body_fill<E>(out, n, cnt, base, static_cast<uint64_t>(delta), lane);
-      pos += 2 + len;
-    } else {
-      cnt = static_cast<uint32_t>(-h);
-      if (n + cnt > cap) { st = CODAG_ECORRUPT; break; }
-      pos += 1;
-      st = body_literals<NSLOT, E>(in, out, n, cnt, pos, end, lane);
-      if (st) break;
-    }
-    n += cnt;
-    __syncwarp();
-    out.flush_to(n * E);
   }
   if (!in.drain() && st == CODAG_OK) st = CODAG_ETIMEOUT;
   out.finish(n * E);
@@ -442,7 +449,7 @@ __device__ __forceinline__ int rlev2_header(InRing<NSLOT>& in, OUT& out, uint32_
 // header whose patch width exceeds 64 bits).
 template <int NSLOT>
 __device__ __forceinline__ uint32_t rlev2_size(const InRing<NSLOT>& in, uint32_t p) {
-  const uint32_t w = __byte_perm(in.peek_le32(p), 0, 0x0123);  // bytes p..p+3, first byte on top
+  const uint32_t w = in.peek_be32(p);  // bytes p..p+3, first byte on top
   const uint32_t first = w >> 24;
   const uint32_t len8 = (((w >> 16) & 0x1ffu) + 1u) & 0xffu;
   const uint32_t fbw = v2_width((first >> 1) & 0x1fu);
@@ -504,7 +511,7 @@ __device__ int decode_rlev2_chunk(InRing<NSLOT>& in, OUT& out, uint32_t cap) {
     uint32_t kc = 0, bit = 0, pinfo = 0, pbit = 0;
     uint64_t va = 0, vb = 0;
     if (lane < k) {
-      const uint32_t w = __byte_perm(in.peek_le32(mine), 0, 0x0123);
+      const uint32_t w = in.peek_be32(mine);
       const uint32_t first = w >> 24;
       const uint32_t len8 = (((w >> 16) & 0x1ffu) + 1u) & 0xffu;
       const uint32_t kind = first >> 6;

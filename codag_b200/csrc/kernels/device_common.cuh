@@ -309,7 +309,17 @@ struct InRing {
     const uint32_t sh = (p & 3u) * 8u;
     return sh ? (v >> sh) | (static_cast<uint64_t>(w2) << (64 - sh)) : v;
   }
-  __device__ __forceinline__ uint64_t peek_be64(uint32_t p) const { return bswap64(peek_le64(p)); }
+  // bytes p..p+7 as a big-endian value (byte p on top): two byte permutes of three aligned words
+  __device__ __forceinline__ uint64_t peek_be64(uint32_t p) const {
+    const uint32_t a = p & ~3u, sel = 0x0123u + 0x1111u * (p & 3u);
+    const uint32_t w0 = rd32(a), w1 = rd32(a + 4), w2 = rd32(a + 8);
+    return (static_cast<uint64_t>(__byte_perm(w0, w1, sel)) << 32) | __byte_perm(w1, w2, sel);
+  }
+  // bytes p..p+3 as a big-endian word (byte p on top): one byte permute of two aligned words
+  __device__ __forceinline__ uint32_t peek_be32(uint32_t p) const {
+    const uint32_t a = p & ~3u;
+    return __byte_perm(rd32(a), rd32(a + 4), 0x0123u + 0x1111u * (p & 3u));
+  }
   // bytes p..p+3, little-endian (two aligned loads)
   __device__ __forceinline__ uint32_t peek_le32(uint32_t p) const {
     const uint32_t a = p & ~3u;

@@ -1,0 +1,251 @@
+// GPU encoders: ORC RLE v1 and RLE v2 files in CODAG's layouts (include/codag.h,
+// codag_compress_rlev1/_rlev2).
+//
+// CODAG encodes on the GPU with one thread per chunk (rlev1/encoder.h:1728-1847 setup_deflate_orig
+// / deflate_orig, rlev2/encoder_trans.h:184-357 block_encode_orig driven by compress_gpu_orig
+// :482-564), then scans the stream lengths and moves every stream to its aligned offset.  The
+// same three steps run here as three kernels on the caller's stream:
+//   k_encode_chunks  one thread per chunk runs the shared writer of ../rle_writers.h (the code
+//                    the host producers run, so the bytes are the same) into its own slot of
+//                    the caller's workspace;
+//   k_scan_offsets   one CTA turns the stream lengths into the aligned offsets (blk_off);
+//   k_gather         one warp per chunk copies its stream to its offset with the alignment
+//                    padding zeroed, and fills col_len.
+// Nothing is allocated; a stream that overruns its workspace slot, or a file larger than the
+// caller's output capacity, is reported in *d_status.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../../include/codag.h"
+#include "../rle_writers.h"
+
+namespace {
+
+constexpr uint64_t kOverflow = ~0ull;
+
+// writer output into a fixed slot; bytes past the slot are counted but not stored
+struct DevSink {
+  uint8_t* p;
+  uint64_t cap;
+  uint64_t n;
+  __device__ void put(uint8_t b) {
+    if (n < cap) p[n] = b;
+    n++;
+  }
+  __device__ uint64_t size() const { return n; }
+  __device__ void set(uint64_t i, uint8_t b) {
+    if (i < cap) p[i] = b;
+  }
+};
+
+// element j of one chunk of the input zero padded past in_bytes (d_in is element aligned)
+template <typename T>
+struct PaddedChunk {
+  const uint8_t* in;
+  uint64_t in_bytes;
+  uint64_t base;
+  __device__ T operator()(uint64_t j) const {
+    const uint64_t o = base + j * sizeof(T);
+    if (o + sizeof(T) <= in_bytes) return __ldg(reinterpret_cast<const T*>(in + o));
+    T v = 0;
+    for (uint32_t k = 0; k < sizeof(T); k++)
+      if (o + k < in_bytes) v = static_cast<T>(v | (static_cast<T>(in[o + k]) << (8 * k)));
+    return v;
+  }
+};
+
+// Same integer types as the host producer reads the values with.
+template <typename T>
+struct Wide;
+template <>
+struct Wide<uint8_t> { using T = unsigned char; };
+template <>
+struct Wide<uint16_t> { using T = unsigned short; };
+template <>
+struct Wide<uint32_t> { using T = unsigned int; };
+template <>
+struct Wide<uint64_t> { using T = unsigned long long; };
+
+template <int CODEC, typename T>
+__global__ void __launch_bounds__(32) k_encode_chunks(const uint8_t* __restrict__ in, uint64_t in_bytes,
+                                                      uint64_t chunk_bytes, uint64_t n, uint8_t* __restrict__ scratch,
+                                                      uint64_t slot, uint64_t* __restrict__ lens) {
+  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  DevSink s{scratch + i * slot, slot, 0};
+  using W = typename Wide<T>::T;
+  const PaddedChunk<W> g{in, in_bytes, i * chunk_bytes};
+  const uint64_t cnt = chunk_bytes / sizeof(T);
+  if constexpr (CODEC == CODAG_CODEC_RLEV1) {
+    codag_fmt::RleV1Writer<T, DevSink> w(s);
+    w.encode([&](uint64_t j) { return static_cast<T>(g(j)); }, cnt);
+  } else {
+    codag_fmt::RleV2Writer<DevSink> w(s);
+    w.encode([&](uint64_t j) { return static_cast<uint64_t>(g(j)); }, cnt);
+  }
+  lens[i] = s.n > slot ? kOverflow : s.n;
+}
+
+// blk_off[i] = sum of round_up(lens[k], ALIGN) for k < i, blk_off[n] = the total; one CTA of
+// 1024 threads, each summing a contiguous range.
+template <uint64_t ALIGN>
+__global__ void __launch_bounds__(1024) k_scan_offsets(const uint64_t* __restrict__ lens, uint64_t n,
+                                                       uint64_t* __restrict__ blk_off, int32_t* __restrict__ status) {
+  __shared__ uint64_t part[1024];
+  __shared__ int bad;
+  const uint32_t t = threadIdx.x;
+  if (t == 0) bad = 0;
+  const uint64_t per = (n + 1023) / 1024, a = t * per, b = a + per < n ? a + per : n;
+  uint64_t s = 0;
+  for (uint64_t i = a; i < b; i++) {
+    const uint64_t l = lens[i];
+    if (l == kOverflow) bad = 1;
+    s += (l + ALIGN - 1) / ALIGN * ALIGN;
+  }
+  part[t] = s;
+  __syncthreads();
+  for (uint32_t d = 1; d < 1024; d <<= 1) {  // inclusive scan of the partial sums
+    const uint64_t o = t >= d ? part[t - d] : 0;
+    __syncthreads();
+    part[t] += o;
+    __syncthreads();
+  }
+  uint64_t run = part[t] - s;
+  for (uint64_t i = a; i < b; i++) {
+    blk_off[i] = run;
+    run += (lens[i] + ALIGN - 1) / ALIGN * ALIGN;
+  }
+  if (t == 1023) blk_off[n] = part[1023];
+  if (t == 0 && bad && status) *status = CODAG_ECORRUPT;
+}
+
+// One warp per chunk: stream i goes to out + head + blk_off[i] and is zero padded to ALIGN
+// bytes.  RLE v1 (head 8): the blob starts with the original size.  RLE v2: blk_off[n] is
+// overwritten with the original size.  The file is out_bytes = head + blk_off[n] long.
+template <uint64_t ALIGN, uint32_t HEAD>
+__global__ void __launch_bounds__(256) k_gather(const uint8_t* __restrict__ scratch, uint64_t slot,
+                                                const uint64_t* __restrict__ lens, uint64_t n, uint8_t* __restrict__ out,
+                                                uint64_t capacity, uint64_t* __restrict__ blk_off,
+                                                uint64_t* __restrict__ col_len, uint64_t in_bytes,
+                                                uint64_t* __restrict__ out_bytes, int32_t* __restrict__ status) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t warps = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
+  const uint64_t total = HEAD + blk_off[n];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (out_bytes) *out_bytes = total;
+    if (total > capacity && status) *status = CODAG_ELIMIT;
+    if (HEAD == 8 && capacity >= 8) *reinterpret_cast<uint64_t*>(out) = in_bytes;
+  }
+  if (total > capacity) return;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+    const uint64_t len = lens[i], off = HEAD + blk_off[i];
+    if (lane == 0) col_len[i] = len;
+    if (len == kOverflow) continue;
+    const uint64_t padded = (len + ALIGN - 1) / ALIGN * ALIGN;
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(scratch + i * slot);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(out + off);  // 4-byte aligned: HEAD, ALIGN multiples of 4
+    for (uint64_t w = lane; w < padded / 4; w += 32) {
+      uint32_t v = 0;
+      const uint64_t b0 = 4 * w;
+      if (b0 + 4 <= len) {
+        v = src[w];
+      } else if (b0 < len) {
+        v = src[w] & ((1u << (8 * (len - b0))) - 1u);  // keep the stream's bytes, zero the padding
+      }
+      dst[w] = v;
+    }
+  }
+}
+
+__global__ void k_set_last_offset(uint64_t* blk_off, uint64_t n, uint64_t in_bytes) { blk_off[n] = in_bytes; }
+
+bool valid_elem(int e) { return e == 1 || e == 2 || e == 4 || e == 8; }
+
+uint64_t chunks_of(uint64_t in_bytes, uint64_t chunk_bytes) {
+  return (in_bytes + chunk_bytes * 32 - 1) / (chunk_bytes * 32) * 32;  // rlev1.h:111-112, encoder_trans.h:490
+}
+
+// Workspace slot per chunk: the longest stream a chunk can give, 16-byte aligned.  RLE v1: every
+// value a varint of ceil(8E/7) bytes plus a header per 127 literals; RLE v2: at most 1.25x the
+// input for 64-bit values, taken as 2x plus a margin for every width.
+uint64_t slot_of(int codec, uint64_t chunk_bytes, int e) {
+  const uint64_t cnt = chunk_bytes / static_cast<uint64_t>(e);
+  const uint64_t b = codec == CODAG_CODEC_RLEV1 ? cnt * ((8u * e + 6u) / 7u) + cnt / 127u + 64u : 2u * chunk_bytes + 4096u;
+  return (b + 15u) / 16u * 16u;
+}
+
+template <int CODEC, typename T>
+void launch_encode(const uint8_t* in, uint64_t in_bytes, uint64_t chunk, uint64_t n, uint8_t* scratch, uint64_t slot,
+                   uint64_t* lens, cudaStream_t s) {
+  k_encode_chunks<CODEC, T><<<static_cast<unsigned>((n + 31) / 32), 32, 0, s>>>(in, in_bytes, chunk, n, scratch, slot, lens);
+}
+
+template <int CODEC>
+codag_status compress(const uint8_t* d_in, uint64_t in_bytes, uint64_t chunk, int e, uint8_t* d_out, uint64_t capacity,
+                      uint64_t* d_blk_off, uint64_t* d_col_len, uint64_t* d_out_bytes, int32_t* d_status, void* ws,
+                      uint64_t ws_bytes, cudaStream_t s) {
+  if (!d_in || !d_out || !d_blk_off || !d_col_len || !valid_elem(e) || chunk == 0 || chunk % e || in_bytes == 0 ||
+      chunk >= (1ull << 31) || (reinterpret_cast<uintptr_t>(d_in) % e) || (reinterpret_cast<uintptr_t>(d_out) & 15u))
+    return CODAG_EINVAL;
+  if (CODEC == CODAG_CODEC_RLEV1 && chunk / e < 2) return CODAG_EINVAL;
+  const uint64_t n = chunks_of(in_bytes, chunk), slot = slot_of(CODEC, chunk, e);
+  if (!ws || ws_bytes < codag_compress_workspace_bytes(CODEC, in_bytes, chunk, e) ||
+      (reinterpret_cast<uintptr_t>(ws) & 255u))
+    return CODAG_EINVAL;
+  uint8_t* scratch = static_cast<uint8_t*>(ws);
+  uint64_t* lens = reinterpret_cast<uint64_t*>(scratch + n * slot);
+  if (d_status && cudaMemsetAsync(d_status, 0, sizeof(int32_t), s) != cudaSuccess) return CODAG_ECUDA;
+  switch (e) {
+    case 8: launch_encode<CODEC, uint64_t>(d_in, in_bytes, chunk, n, scratch, slot, lens, s); break;
+    case 4: launch_encode<CODEC, uint32_t>(d_in, in_bytes, chunk, n, scratch, slot, lens, s); break;
+    case 2: launch_encode<CODEC, uint16_t>(d_in, in_bytes, chunk, n, scratch, slot, lens, s); break;
+    default: launch_encode<CODEC, uint8_t>(d_in, in_bytes, chunk, n, scratch, slot, lens, s); break;
+  }
+  constexpr uint64_t A = CODEC == CODAG_CODEC_RLEV1 ? 4 : 128;  // encoder.h:780-783 / encoder_trans.h:352
+  constexpr uint32_t H = CODEC == CODAG_CODEC_RLEV1 ? 8 : 0;    // rlev1.h:103-192: [u64 size][streams]
+  k_scan_offsets<A><<<1, 1024, 0, s>>>(lens, n, d_blk_off, d_status);
+  const uint64_t blocks = (n + 7) / 8;
+  k_gather<A, H><<<static_cast<unsigned>(blocks < 4096 ? blocks : 4096), 256, 0, s>>>(
+      scratch, slot, lens, n, d_out, capacity, d_blk_off, d_col_len, in_bytes, d_out_bytes, d_status);
+  if (CODEC == CODAG_CODEC_RLEV2) k_set_last_offset<<<1, 1, 0, s>>>(d_blk_off, n, in_bytes);  // encoder_trans.h:545
+  return cudaGetLastError() == cudaSuccess ? CODAG_OK : CODAG_ECUDA;
+}
+
+}  // namespace
+
+extern "C" uint64_t codag_compress_chunks(uint64_t in_bytes, uint64_t chunk_bytes) {
+  return chunk_bytes ? chunks_of(in_bytes, chunk_bytes) : 0;
+}
+
+extern "C" uint64_t codag_compress_workspace_bytes(int codec, uint64_t in_bytes, uint64_t chunk_bytes, int elem_bytes) {
+  if ((codec != CODAG_CODEC_RLEV1 && codec != CODAG_CODEC_RLEV2) || !valid_elem(elem_bytes) || !chunk_bytes) return 0;
+  const uint64_t n = chunks_of(in_bytes, chunk_bytes);
+  return n * slot_of(codec, chunk_bytes, elem_bytes) + n * 8;
+}
+
+extern "C" uint64_t codag_compress_bound(int codec, uint64_t in_bytes, uint64_t chunk_bytes, int elem_bytes) {
+  if ((codec != CODAG_CODEC_RLEV1 && codec != CODAG_CODEC_RLEV2) || !valid_elem(elem_bytes) || !chunk_bytes) return 0;
+  const uint64_t n = chunks_of(in_bytes, chunk_bytes), slot = slot_of(codec, chunk_bytes, elem_bytes);
+  return codec == CODAG_CODEC_RLEV1 ? 8 + n * ((slot + 3) / 4 * 4) : n * ((slot + 127) / 128 * 128);
+}
+
+extern "C" codag_status codag_compress_rlev1(const uint8_t* d_in, uint64_t in_bytes, uint64_t chunk_bytes,
+                                             int elem_bytes, uint8_t* d_blob, uint64_t blob_capacity,
+                                             uint64_t* d_blk_off, uint64_t* d_col_len, uint64_t* d_blob_bytes,
+                                             int32_t* d_status, void* d_workspace, uint64_t workspace_bytes,
+                                             codag_stream_t stream) {
+  return compress<CODAG_CODEC_RLEV1>(d_in, in_bytes, chunk_bytes, elem_bytes, d_blob, blob_capacity, d_blk_off,
+                                     d_col_len, d_blob_bytes, d_status, d_workspace, workspace_bytes,
+                                     reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" codag_status codag_compress_rlev2(const uint8_t* d_in, uint64_t in_bytes, uint64_t chunk_bytes,
+                                             int elem_bytes, uint8_t* d_comp, uint64_t comp_capacity,
+                                             uint64_t* d_blk_off, uint64_t* d_col_len, uint64_t* d_comp_bytes,
+                                             int32_t* d_status, void* d_workspace, uint64_t workspace_bytes,
+                                             codag_stream_t stream) {
+  return compress<CODAG_CODEC_RLEV2>(d_in, in_bytes, chunk_bytes, elem_bytes, d_comp, comp_capacity, d_blk_off,
+                                     d_col_len, d_comp_bytes, d_status, d_workspace, workspace_bytes,
+                                     reinterpret_cast<cudaStream_t>(stream));
+}

@@ -27,11 +27,13 @@ EXPORTS = (
     "codag_decompress_rlev2_noalloc",
     "codag_set_tune", "codag_get_tune", "codag_set_wait_limit", "codag_selftest_wait_timeout",
     "codag_batch_plan", "codag_batch_run", "codag_batch_destroy", "codag_batch_launch",
+    "codag_compress_chunks", "codag_compress_bound", "codag_compress_workspace_bytes",
+    "codag_compress_rlev1", "codag_compress_rlev2",
 )
 # every symbol declared in include/codag_format.h (libcodag_fmt.so)
 FMT_EXPORTS = (
     "codag_hbuf_free", "codag_encode_rlev1", "codag_encode_rlev2", "codag_encode_deflate", "codag_encode_one",
-    "codag_encode_set",
+    "codag_encode_set", "codag_encode_cudf_deflate", "codag_cudf_deflate_layout",
     "codag_gen_rlev1_column", "codag_gen_rlev2_column", "codag_gen_text",
 )
 
@@ -91,6 +93,14 @@ def lib() -> C.CDLL:
     L.codag_batch_run.argtypes = [vp, vp, u64, vp, u64, vp, C.c_int, vp]
     L.codag_batch_destroy.argtypes = [vp]
     L.codag_batch_launch.argtypes = [vp, vp, u64, vp, C.POINTER(Tune), vp, u64, vp, u64, vp, vp]
+    L.codag_compress_chunks.argtypes = [u64, u64]
+    L.codag_compress_chunks.restype = u64
+    for name in ("codag_compress_bound", "codag_compress_workspace_bytes"):
+        getattr(L, name).argtypes = [C.c_int, u64, u64, C.c_int]
+        getattr(L, name).restype = u64
+    for name in ("codag_compress_rlev1", "codag_compress_rlev2"):
+        getattr(L, name).argtypes = [vp, u64, u64, C.c_int, vp, u64, vp, vp, vp, vp, vp, u64, vp]
+        getattr(L, name).restype = i32
     for name in ("codag_set_tune", "codag_get_tune", "codag_set_wait_limit", "codag_selftest_wait_timeout",
                  "codag_batch_plan", "codag_batch_run", "codag_batch_destroy", "codag_batch_launch"):
         getattr(L, name).restype = i32
@@ -116,8 +126,10 @@ def fmt_lib() -> C.CDLL:
                                        C.POINTER(HBuf)]
     L.codag_encode_one.argtypes = [C.c_int, vp, u64, C.c_int, C.c_int, C.POINTER(HBuf)]
     L.codag_encode_set.argtypes = [vp, vp, vp, vp, vp, u64, C.c_int, vp, C.POINTER(HBuf), C.POINTER(u64)]
+    L.codag_encode_cudf_deflate.argtypes = [vp, u64, u64, C.c_int, C.POINTER(HBuf)]
+    L.codag_cudf_deflate_layout.argtypes = [vp, u64, C.POINTER(u64), C.POINTER(u64), C.POINTER(u64), vp]
     for name in ("codag_encode_rlev1", "codag_encode_rlev2", "codag_encode_deflate", "codag_encode_one",
-                 "codag_encode_set"):
+                 "codag_encode_set", "codag_encode_cudf_deflate", "codag_cudf_deflate_layout"):
         getattr(L, name).restype = i32
     for name in ("codag_gen_rlev1_column", "codag_gen_rlev2_column"):
         getattr(L, name).argtypes = [u64, u64, C.c_int, vp]
@@ -178,6 +190,27 @@ def encode_deflate(data: np.ndarray, chunk_bytes: int = 131072, level: int = 6, 
                                                             int(zlib_wrapper), int(require_no_stored),
                                                             C.byref(b1), C.byref(b2), C.byref(b3)))
     return _take(b1), _take(b2, np.uint64), _take(b3, np.uint64)
+
+
+def encode_cudf_deflate(data: np.ndarray, chunk_bytes: int = 65536, level: int = 9) -> np.ndarray:
+    """CODAG's cuDF-comparison file (codag_encode_cudf_deflate) as one byte array."""
+    raw = np.ascontiguousarray(data).view(np.uint8).reshape(-1)
+    b = HBuf()
+    check("codag_encode_cudf_deflate", fmt_lib().codag_encode_cudf_deflate(_ptr(raw), raw.nbytes, chunk_bytes, level,
+                                                                           C.byref(b)))
+    return _take(b)
+
+
+def cudf_deflate_layout(file: np.ndarray):
+    """(chunk_bytes, data_offset, blk_off[n+1] relative to data_offset) of a cuDF-comparison file."""
+    raw = np.ascontiguousarray(file).view(np.uint8).reshape(-1)
+    ch, n, off = C.c_uint64(), C.c_uint64(), C.c_uint64()
+    check("codag_cudf_deflate_layout", fmt_lib().codag_cudf_deflate_layout(_ptr(raw), raw.nbytes, C.byref(ch), C.byref(n),
+                                                                           C.byref(off), None))
+    blk = np.zeros(n.value + 1, np.uint64)
+    check("codag_cudf_deflate_layout", fmt_lib().codag_cudf_deflate_layout(_ptr(raw), raw.nbytes, C.byref(ch), C.byref(n),
+                                                                           C.byref(off), _ptr(blk)))
+    return int(ch.value), int(off.value), blk
 
 
 def encode_one(codec: int, data: np.ndarray, elem_bytes: int = 8, level: int = 6) -> np.ndarray:

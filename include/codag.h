@@ -121,6 +121,36 @@ codag_status codag_decompress_deflate(const uint8_t *d_comp, uint64_t comp_bytes
                                       uint64_t out_bytes, int32_t *d_chunk_status,
                                       codag_stream_t stream);
 
+/* --- GPU encoders -----------------------------------------------------------------------
+ * CODAG's rlev1/rlev2 tools encode on the GPU, one thread per chunk, before they decode
+ * (rle_v1::compress_gpu_orig, include/rlev1/rlev1.h:103-192 with rlev1/encoder.h:1728-1847;
+ * rlev2::compress_gpu_orig, include/rlev2/encoder_trans.h:482-564).  These write the same
+ * files, byte for byte, as the host producers of codag_format.h (codag_encode_rlev1/_rlev2),
+ * from a column in device memory, asynchronously on `stream`, allocating nothing:
+ *   n = codag_compress_chunks(in_bytes, chunk_bytes) chunks (a multiple of 32, the input zero
+ *       padded to n * chunk_bytes);
+ *   d_blk_off  n+1 u64: RLE v1 stream i at d_blob + 8 + d_blk_off[i] (4-byte aligned),
+ *              RLE v2 stream i at d_comp + d_blk_off[i] (128-byte aligned), d_blk_off[n] = in_bytes;
+ *   d_col_len  n u64 exact stream lengths;
+ *   d_blob/d_comp  16-byte aligned, capacity bytes (codag_compress_bound always suffices);
+ *              the RLE v1 blob starts with the u64 original size;
+ *   d_out_bytes    (nullable) receives the file length in bytes;
+ *   d_status       (nullable) receives CODAG_OK, CODAG_ELIMIT (capacity too small: nothing
+ *              written) or CODAG_ECORRUPT (a stream outgrew its workspace slot);
+ *   d_workspace    codag_compress_workspace_bytes(...) bytes, 256-byte aligned; d_in is
+ *              aligned to elem_bytes. */
+uint64_t codag_compress_chunks(uint64_t in_bytes, uint64_t chunk_bytes);
+uint64_t codag_compress_bound(int codec, uint64_t in_bytes, uint64_t chunk_bytes, int elem_bytes);
+uint64_t codag_compress_workspace_bytes(int codec, uint64_t in_bytes, uint64_t chunk_bytes, int elem_bytes);
+codag_status codag_compress_rlev1(const uint8_t *d_in, uint64_t in_bytes, uint64_t chunk_bytes, int elem_bytes,
+                                  uint8_t *d_blob, uint64_t blob_capacity, uint64_t *d_blk_off,
+                                  uint64_t *d_col_len, uint64_t *d_out_bytes, int32_t *d_status,
+                                  void *d_workspace, uint64_t workspace_bytes, codag_stream_t stream);
+codag_status codag_compress_rlev2(const uint8_t *d_in, uint64_t in_bytes, uint64_t chunk_bytes, int elem_bytes,
+                                  uint8_t *d_comp, uint64_t comp_capacity, uint64_t *d_blk_off,
+                                  uint64_t *d_col_len, uint64_t *d_out_bytes, int32_t *d_status,
+                                  void *d_workspace, uint64_t workspace_bytes, codag_stream_t stream);
+
 /* --- launch tuning --------------------------------------------------------------------
  * Process-wide launch shape for the per-file calls above, per codec.  warps_per_cta is
  * the number of chunks one CTA decodes (one warp per chunk, 1..8); ring_slots the depth of

@@ -42,6 +42,17 @@ codag_status codag_encode_rlev2(const uint8_t *in, uint64_t in_bytes, uint64_t c
 codag_status codag_encode_deflate(const uint8_t *in, uint64_t in_bytes, uint64_t chunk_bytes,
                                   int level, int zlib_wrapper, int require_no_stored,
                                   codag_hbuf *comp, codag_hbuf *blk_offset, codag_hbuf *col_len);
+/* CODAG's cuDF-comparison layout (rapids_compressor.py:222-275, read by
+ * include/base_deflate.h:20-130): file = [u64 chunk_bytes][u64 n][u64 size_i x n] then the n
+ * zlib-wrapped streams back to back, one per chunk of the input zero padded to a multiple of
+ * chunk_bytes (the script uses 64 KiB chunks and level 9).  Decode with
+ * codag_decompress_deflate(file + data_offset, ..., blk_off, n, chunk_bytes, wrapper_bytes = 2). */
+codag_status codag_encode_cudf_deflate(const uint8_t *in, uint64_t in_bytes, uint64_t chunk_bytes,
+                                       int level, codag_hbuf *file);
+/* Parses that layout: chunk size, chunk count, byte offset of the first stream, and (blk_off
+ * non-NULL) n+1 stream offsets relative to it.  CODAG_EINVAL if a size runs past the file. */
+codag_status codag_cudf_deflate_layout(const uint8_t *file, uint64_t file_bytes, uint64_t *chunk_bytes,
+                                       uint64_t *n_chunks, uint64_t *data_offset, uint64_t *blk_off);
 /* One stream of a single buffer (the batched workload's per-chunk files). */
 codag_status codag_encode_one(int codec, const uint8_t *in, uint64_t in_bytes, int elem_bytes,
                               int level, codag_hbuf *stream);

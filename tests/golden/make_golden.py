@@ -1,10 +1,13 @@
-"""Regenerates the golden files of tests/golden from CODAG's own Python compressor.
+"""Regenerates the golden files of tests/golden from CODAG's own Python compressors.
 
 Runs only where the CODAG tree is available: give it with --ref or $CODAG_REFERENCE_DIR.
 deflate_compressor.py imports `zstandard` at module level without using it on this path,
 and writes to a hard-coded directory; the script stubs the first and redirects the second
 into this folder, then calls CODAG's zlib_chunk_compress (deflate_compressor.py:44-125)
-on a seeded text sample.  The tests compare our layout writer against these files.
+on a seeded text sample; likewise rapids_compressor.py's zlib_chunk_compress
+(rapids_compressor.py:222-275, the layout of CODAG's cuDF comparison, 64 KiB chunks at zlib
+level 9), which writes output/comp3.bin under the working directory, run in a temporary
+directory.  The tests compare our layout writers against these files.
 
     CODAG_REFERENCE_DIR=<CODAG tree> python tests/golden/make_golden.py
 """
@@ -47,6 +50,22 @@ def main() -> None:
     dc.zlib_chunk_compress(src.tobytes(), "deflate_ref")
     for name in ("deflate_ref_comp.bin", "deflate_ref_blk_offset.bin", "deflate_ref_col_len.bin"):
         print(name, (HERE / name).stat().st_size)
+
+    import tempfile
+    import rapids_compressor as rc  # CODAG's cuDF-comparison compressor
+    rc.print = lambda *a, **k: None
+    cudf_src = native.gen_text(200_000, 434343)
+    (HERE / "cudf_src.bin").write_bytes(cudf_src.tobytes())
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as td:
+        os.chdir(td)
+        try:
+            os.mkdir("output")
+            rc.zlib_chunk_compress(cudf_src.tobytes())
+            (HERE / "cudf_ref_comp.bin").write_bytes(Path(td, "output", "comp3.bin").read_bytes())
+        finally:
+            os.chdir(cwd)
+    print("cudf_ref_comp.bin", (HERE / "cudf_ref_comp.bin").stat().st_size)
 
 
 if __name__ == "__main__":
