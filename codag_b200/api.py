@@ -127,6 +127,17 @@ def compress_rle(codec: int, col: torch.Tensor, chunk_bytes: int = 131072, elem_
     return out[:nbytes], blk_off, col_len
 
 
+def decompress_rlev2_transposed(comp: torch.Tensor, blk_off: torch.Tensor, col_len: torch.Tensor, chunk_bytes: int,
+                                elem_bytes: int, read_unit: int, out: torch.Tensor, out_bytes: int | None = None,
+                                status: torch.Tensor | None = None, stream=None) -> None:
+    """codag_decompress_rlev2_transposed: CODAG's transposed RLE v2 layout (blk_off: n chunk
+    offsets, col_len: 32 substream lengths per chunk) into `out`."""
+    n = blk_off.numel()
+    check("codag_decompress_rlev2_transposed", native.lib().codag_decompress_rlev2_transposed(
+        _dptr(comp), comp.numel(), _dptr(blk_off), _dptr(col_len), n, chunk_bytes, elem_bytes, read_unit, _dptr(out),
+        out.numel() if out_bytes is None else out_bytes, _dptr(status), _stream(stream)))
+
+
 def selftest_wait_timeout(wait_cycles: int = 2_000_000) -> int:
     """Runs the bounded-wait self test and returns the status it reports (expect ETIMEOUT)."""
     native.set_wait_limit(wait_cycles)
@@ -324,73 +335,72 @@ class BatchPlan:
 
 class BatchHostPipeline:
     """Decodes a packed set of independent files (codag_batch_plan descriptors) from pinned host
-    memory into pinned host memory, overlapping the copies with the decode.
+    memory into pinned host memory, one set per step, with the steps pipelined.
 
-    The files are split into `groups` of about equal decode cost (Deflate bytes weigh more),
-    each with its own persistent plan; group g's compressed bytes go up, its launch runs and
-    its outputs come down on stream g % streams, so one group's host-to-device copy, another
-    group's decode and a third group's device-to-host copy overlap, and the launches of
-    different groups overlap on the GPU as well (a launch ends with its longest file while the
-    next one fills the other SMs).  Files must be packed in index order, as pack_chunks and
-    codag_encode_set do, so each group's input and output are contiguous ranges; the output
-    ranges tile the whole output buffer.  Device buffers and plans live as long as the
-    pipeline; bytes between and after the files' outputs come back as zeros."""
+    Two device buffer pairs alternate between steps, and three streams carry the stages: step
+    i's host-to-device copy runs while step i-1 decodes (one persistent launch, replayed from a
+    CUDA graph captured per buffer pair) and step i-2's output goes back to the host, so a
+    stream of steps runs at the pace of the slowest stage rather than the sum of the three.
+    Events order the reuse of a buffer pair: its input is overwritten only after the launch
+    that read it, its output only after the copy that read it.  Bytes between and after the
+    files' outputs come back as zeros."""
 
-    def __init__(self, descs: np.ndarray, comp_bytes: int, out_bytes: int, groups: int = 6, streams: int = 3,
-                 shape: tuple | None = None, device="cuda"):
+    def __init__(self, descs: np.ndarray, comp_bytes: int, out_bytes: int, shape: tuple | None = None,
+                 device="cuda", buffers: int = 2):
         descs = np.ascontiguousarray(descs, dtype=native.CHUNK_DESC_DTYPE)
-        n = descs.size
+        self.n = descs.size
         self.dev = torch.device(device)
-        cost = descs["out_len"].astype(np.int64) + np.where(descs["codec"] == native.DEFLATE, 8, 1) * \
-            descs["comp_len"].astype(np.int64)
-        cum = np.cumsum(cost)
-        cuts = np.searchsorted(cum, np.linspace(0, cum[-1], min(groups, n) + 1)[1:-1], side="right")
-        bounds = np.unique(np.concatenate([[0], cuts, [n]]))
-        self.groups = []
-        for a, b in zip(bounds[:-1], bounds[1:]):
-            d = descs[a:b]
-            self.groups.append(dict(
-                a=int(a), b=int(b), plan=BatchPlan(d, *(shape or ())),
-                c0=int(d["comp_off"].min()), c1=int((d["comp_off"] + d["comp_len"]).max()),
-                o0=int(d["out_off"].min()), o1=int((d["out_off"] + d["out_len"]).max())))
-        # output ranges tile [0, out_bytes): the bytes between and after files come back as zeros
-        for k, g in enumerate(self.groups):
-            g["o0"] = 0 if k == 0 else self.groups[k - 1]["o1"]
-            if k == len(self.groups) - 1:
-                g["o1"] = max(out_bytes, g["o1"])
-        self.d_comp = torch.empty(max(comp_bytes, 1), dtype=torch.uint8, device=self.dev)
-        self.d_out = torch.zeros(max(out_bytes, 1), dtype=torch.uint8, device=self.dev)
-        self.d_st = torch.zeros(max(n, 1), dtype=torch.int32, device=self.dev)
-        self.streams = [torch.cuda.Stream(device=self.dev) for _ in range(streams)]
+        self.comp_bytes, self.out_bytes = comp_bytes, out_bytes
+        # one plan per buffer pair, so that each keeps the graph captured for its pointers
+        self.bufs = [dict(plan=BatchPlan(descs, *(shape or ())),
+                          comp=torch.empty(max(comp_bytes, 1), dtype=torch.uint8, device=self.dev),
+                          out=torch.zeros(max(out_bytes, 1), dtype=torch.uint8, device=self.dev),
+                          st=torch.zeros(max(self.n, 1), dtype=torch.int32, device=self.dev),
+                          decoded=None, copied=None) for _ in range(buffers)]
+        self.s_in, self.s_dec, self.s_out = (torch.cuda.Stream(device=self.dev) for _ in range(3))
 
-    @property
-    def h2d_bytes(self) -> int:
-        return sum(g["c1"] - g["c0"] for g in self.groups)
+    h2d_bytes = property(lambda self: self.comp_bytes)
+    d2h_bytes = property(lambda self: self.out_bytes)
 
-    @property
-    def d2h_bytes(self) -> int:
-        return sum(g["o1"] - g["o0"] for g in self.groups)
-
-    def run(self, h_comp: torch.Tensor, h_out: torch.Tensor, use_graph: bool = True) -> None:
-        """h_comp/h_out pinned uint8 covering the set's input and output.  Returns after every
-        output is in h_out; raises CodagError with the per-file status if a file failed."""
+    def run(self, steps, use_graph: bool = True) -> None:
+        """steps: (h_comp, h_out) pairs of pinned uint8 tensors, one per step.  Returns after
+        every output is in its h_out; raises CodagError with the per-file status if a file
+        failed in any step."""
         main = torch.cuda.current_stream(self.dev)
-        for s in self.streams:
+        for s in (self.s_in, self.s_dec, self.s_out):
             s.wait_stream(main)
-        for k, g in enumerate(self.groups):
-            s = self.streams[k % len(self.streams)]
-            with torch.cuda.stream(s):
-                self.d_comp[g["c0"]:g["c1"]].copy_(h_comp[g["c0"]:g["c1"]], non_blocking=True)
-                g["plan"].run(self.d_comp, self.d_out, self.d_st[g["a"]:g["b"]], use_graph=use_graph, stream=s)
-                h_out[g["o0"]:g["o1"]].copy_(self.d_out[g["o0"]:g["o1"]], non_blocking=True)
-        for s in self.streams:
+        bad = []
+        for i, (h_comp, h_out) in enumerate(steps):
+            b = self.bufs[i % len(self.bufs)]
+            if b["decoded"] is not None:
+                self.s_in.wait_event(b["decoded"])   # the previous launch on this pair read its input
+            with torch.cuda.stream(self.s_in):
+                b["comp"].copy_(h_comp[:self.comp_bytes], non_blocking=True)
+            ready = torch.cuda.Event()
+            ready.record(self.s_in)
+            self.s_dec.wait_event(ready)
+            if b["copied"] is not None:
+                self.s_dec.wait_event(b["copied"])   # the previous copy-out of this pair is done
+            with torch.cuda.stream(self.s_dec):
+                b["plan"].run(b["comp"], b["out"], b["st"], use_graph=use_graph, stream=self.s_dec)
+                bad.append((b["st"] != 0).any())
+            b["decoded"] = torch.cuda.Event()
+            b["decoded"].record(self.s_dec)
+            self.s_out.wait_event(b["decoded"])
+            with torch.cuda.stream(self.s_out):
+                h_out[:self.out_bytes].copy_(b["out"], non_blocking=True)
+            b["copied"] = torch.cuda.Event()
+            b["copied"].record(self.s_out)
+        for s in (self.s_in, self.s_dec, self.s_out):
             main.wait_stream(s)
         main.synchronize()
-        _status_error("BatchHostPipeline", self.d_st)
+        if any(bool(x) for x in bad):
+            for b in self.bufs:
+                _status_error("BatchHostPipeline", b["st"])
 
     def close(self) -> None:
-        for g in self.groups:
-            g["plan"].close()
+        for b in self.bufs:
+            b["plan"].close()
 
 
 @dataclass

@@ -30,7 +30,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fop
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fopenmp", "-Wall", "-Wno-unused-function"]
 
 HOST_SOURCES = sorted((CSRC / "host").glob("*.cpp"))
-CUDA_SOURCES = [CSRC / "kernels" / "codag_capi.cu", CSRC / "kernels" / "encode_capi.cu"]
+CUDA_SOURCES = [CSRC / "kernels" / name for name in ("codag_capi.cu", "encode_capi.cu", "transposed_capi.cu")]
 CUDA = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 HEADERS = (sorted(CSRC.rglob("*.cuh")) + sorted(CSRC.rglob("*.hpp")) + sorted(CSRC.glob("*.h")) +
            [REPO / "include" / "codag.h", REPO / "include" / "codag_format.h"])

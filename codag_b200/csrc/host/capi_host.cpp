@@ -7,6 +7,7 @@
 #include <cstring>
 #include <vector>
 
+#include "../rle_writers.h"
 #include "host_common.hpp"
 
 using namespace codag_host;
@@ -137,6 +138,77 @@ extern "C" codag_status codag_encode_deflate(const uint8_t* in, uint64_t in_byte
     pos += len[i];
   }
   if (!to_hbuf(out.data(), out.size(), comp) || !to_hbuf(off.data(), off.size() * 8, blk_offset) ||
+      !to_hbuf(len.data(), len.size() * 8, col_len))
+    return CODAG_ENOMEM;
+  return CODAG_OK;
+}
+
+// CODAG's transposed RLE v2 layout (rlev2::compress_gpu_transpose, include/rlev2/encoder_trans.h:
+// 8-182 block_encode and 359-391 tranpose_col_len_single).  Chunk c of the input (zero padded to
+// a multiple of chunk_bytes; no padding of the chunk count) is split into 32 substreams:
+// substream t holds the values t*ru + k*32*ru + j (0 <= j < ru), each encoded on its own.  The
+// chunk's region starts at blk_off[c] and interleaves the substreams in 4-byte words: for
+// w = 0, 1, ... every substream still longer than 4w contributes its bytes [4w, 4w+4), in
+// substream order.  The bytes of such a word past a substream's end are the bytes that follow
+// it when all substreams of all chunks are laid end to end (zero past the last one), which is
+// what CODAG's copy reads.  A region is round_up(sum of round_up4(length), 128) bytes (zero
+// filled), blk_off[n] holds the original size, col_len the 32 exact lengths per chunk.
+extern "C" codag_status codag_encode_rlev2_transposed(const uint8_t* in, uint64_t in_bytes, uint64_t chunk_bytes,
+                                                      int elem_bytes, int read_unit, codag_hbuf* comp,
+                                                      codag_hbuf* blk_off, codag_hbuf* col_len) {
+  if (!in || !comp || !blk_off || !col_len || !valid_elem(elem_bytes) || chunk_bytes == 0 || in_bytes == 0 ||
+      read_unit <= 0 || chunk_bytes % (static_cast<uint64_t>(elem_bytes) * 32u * static_cast<uint64_t>(read_unit)))
+    return CODAG_EINVAL;
+  const uint64_t n = (in_bytes + chunk_bytes - 1) / chunk_bytes;
+  std::vector<uint8_t> padded(n * chunk_bytes, 0);
+  std::memcpy(padded.data(), in, in_bytes);
+  const uint64_t per = chunk_bytes / elem_bytes / 32, ru = static_cast<uint64_t>(read_unit);
+  std::vector<std::vector<uint8_t>> subs(n * 32);
+#pragma omp parallel for schedule(dynamic, 32)
+  for (int64_t f = 0; f < static_cast<int64_t>(n * 32); f++) {
+    const uint64_t c = f / 32, t = f % 32;
+    const uint8_t* base = padded.data() + c * chunk_bytes;
+    VectorSink sink{subs[f]};
+    codag_fmt::RleV2Writer<VectorSink> w(sink);
+    w.encode([&](uint64_t j) {
+      const uint64_t e = t * ru + (j / ru) * 32 * ru + j % ru;
+      uint64_t v = 0;
+      std::memcpy(&v, base + e * elem_bytes, elem_bytes);
+      return v;
+    }, per);
+  }
+  // all substreams end to end (the source of the interleaved words)
+  std::vector<uint64_t> acc(n * 32 + 1, 0);
+  for (uint64_t f = 0; f < n * 32; f++) acc[f + 1] = acc[f] + subs[f].size();
+  std::vector<uint8_t> packed(acc[n * 32] + 4, 0);
+  for (uint64_t f = 0; f < n * 32; f++) std::memcpy(packed.data() + acc[f], subs[f].data(), subs[f].size());
+  std::vector<uint64_t> off(n + 1, 0), len(n * 32, 0);
+  for (uint64_t c = 0; c < n; c++) {
+    uint64_t words = 0;
+    for (uint64_t t = 0; t < 32; t++) {
+      len[c * 32 + t] = subs[c * 32 + t].size();
+      words += (len[c * 32 + t] + 3) / 4;
+    }
+    off[c + 1] = off[c] + round_up(4 * words, 128);
+  }
+  std::vector<uint8_t> out(off[n], 0);
+  for (uint64_t c = 0; c < n; c++) {
+    uint64_t o = off[c];
+    for (uint64_t w = 0;; w++) {
+      bool any = false;
+      for (uint64_t t = 0; t < 32; t++) {
+        const uint64_t f = c * 32 + t;
+        if (len[f] > 4 * w) {
+          std::memcpy(out.data() + o, packed.data() + acc[f] + 4 * w, 4);
+          o += 4;
+          any = true;
+        }
+      }
+      if (!any) break;
+    }
+  }
+  off[n] = in_bytes;  // the last entry carries the original size (encoder_trans.h:460)
+  if (!to_hbuf(out.data(), out.size(), comp) || !to_hbuf(off.data(), off.size() * 8, blk_off) ||
       !to_hbuf(len.data(), len.size() * 8, col_len))
     return CODAG_ENOMEM;
   return CODAG_OK;

@@ -1,0 +1,282 @@
+// Decoder of CODAG's transposed RLE v2 layout (include/codag.h, codag_decompress_rlev2_transposed).
+//
+// In that layout (include/rlev2/encoder_trans.h:8-182 and 359-391) a chunk is 32 substreams,
+// substream t holding the values t*ru + k*32*ru + j (j < ru), and the chunk's bytes interleave
+// the substreams in 4-byte words: word w of every substream longer than 4w, in substream
+// order, then word w+1.  CODAG decodes it with one lane per substream fed by a reader warp
+// through spin queues (include/rlev2/decoder_new.h:375-632, 1193-1230).  Here one warp
+// decodes a chunk with no queue: the warp first tabulates, per word index w, the mask of
+// substreams that still have a word w and the number of words before row w (shared memory),
+// so lane t finds its word w at row_start[w] + popc(mask[w] & lanes below t) by itself; then
+// every lane decodes its own substream and writes its values straight to their interleaved
+// places in global memory.  Header semantics are CODAG's (the oracle's restatement of
+// decoder_new.h:1000-1184, quirks included: the uint8_t run length, the 32-bit patch mask, the
+// arithmetic-shift zigzag and the DELTA direction taken from the base delta).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../../include/codag.h"
+#include "../rlev2_widths.h"
+
+namespace {
+
+constexpr uint32_t FULL = 0xffffffffu;
+
+__device__ __forceinline__ uint64_t shl64(uint64_t v, uint32_t s) { return s >= 64 ? 0ull : v << s; }
+__device__ __forceinline__ uint64_t shr64(uint64_t v, uint32_t s) { return s >= 64 ? 0ull : v >> s; }
+
+// bytes of one lane's substream, read word by word from the interleaved region
+struct LaneReader {
+  const uint32_t* region;  // the chunk's region (128-byte aligned)
+  const uint32_t* mask;    // shared: substreams with a word at each row
+  const uint32_t* start;   // shared: words before each row
+  uint32_t lt;             // lanes below this one
+  uint32_t len;            // substream bytes
+  uint32_t p;              // next byte
+  uint32_t cw, cv;         // cached word index and value
+  bool bad;
+
+  __device__ __forceinline__ uint32_t byte() {
+    if (p >= len) {
+      bad = true;
+      return 0;
+    }
+    const uint32_t w = p >> 2;
+    if (w != cw) {
+      cw = w;
+      cv = __ldg(region + start[w] + __popc(mask[w] & lt));
+    }
+    return (cv >> (8u * (p++ & 3u))) & 0xffu;
+  }
+};
+
+// MSB-first bits local to one header (decoder_new.h:1024-1040)
+struct HeaderBits {
+  uint32_t cur, left;
+  __device__ __forceinline__ uint64_t read(LaneReader& r, uint32_t n) {
+    uint64_t v = 0;
+    while (n > left) {
+      v = shl64(v, left) | (cur & ((1u << left) - 1u));
+      n -= left;
+      cur = r.byte();
+      left = 8;
+    }
+    if (n) {
+      v = shl64(v, n);
+      left -= n;
+      v |= (cur >> left) & ((1u << n) - 1u);
+    }
+    return v;
+  }
+};
+
+// value k of substream t lands on element t*ru + (k/ru)*32*ru + k%ru of the chunk
+template <typename T>
+struct LaneOut {
+  T* chunk;
+  uint32_t t, ru, cap, store;  // cap: values per substream; store: elements of the chunk to store
+  uint32_t n;
+  bool over;
+  __device__ __forceinline__ uint32_t elem(uint32_t k) const { return t * ru + (k / ru) * 32u * ru + k % ru; }
+  __device__ __forceinline__ void put(uint64_t v) {
+    if (n >= cap) {
+      over = true;
+      return;
+    }
+    const uint32_t e = elem(n++);
+    if (e < store) chunk[e] = static_cast<T>(v);
+  }
+  __device__ __forceinline__ uint64_t get(uint32_t k) const {
+    const uint32_t e = elem(k);
+    return e < store ? static_cast<uint64_t>(chunk[e]) : 0ull;
+  }
+  __device__ __forceinline__ void set(uint32_t k, uint64_t v) {
+    const uint32_t e = elem(k);
+    if (e < store) chunk[e] = static_cast<T>(v);
+  }
+};
+
+__device__ __forceinline__ uint64_t uvarint(LaneReader& r) {
+  uint64_t v = 0;
+  uint32_t off = 0, b;
+  do {
+    b = r.byte();
+    if (r.bad) return 0;
+    v |= shl64(b & 0x7fu, off);
+    off += 7;
+  } while (b >= 0x80u);
+  return v;
+}
+
+template <typename T>
+__device__ int decode_substream(LaneReader& r, LaneOut<T>& o) {
+  constexpr uint64_t M = sizeof(T) == 8 ? ~0ull : ((1ull << (8 * sizeof(T))) - 1ull);
+  while (r.p < r.len) {
+    const uint32_t first = r.byte();
+    switch (first & 0xC0u) {
+      case 0x00: {  // SHORT_REPEAT (decoder_new.h:1004-1014)
+        uint32_t nb = ((first >> 3) & 7u) + 1u, cnt = (first & 7u) + 3u;
+        uint64_t v = 0;
+        while (nb-- > 0) v |= shl64(r.byte(), nb * 8u);
+        while (cnt-- > 0) o.put(v & M);
+      } break;
+      case 0x40: {  // DIRECT (decoder_new.h:1015-1043)
+        const uint32_t fbw = v2_width((first >> 1) & 0x1fu);
+        uint8_t len = static_cast<uint8_t>((((first & 1u) << 8) | r.byte()) + 1u);
+        HeaderBits b{0, 0};
+        while (len-- > 0) o.put(b.read(r, fbw) & M);
+      } break;
+      case 0xC0: {  // DELTA (decoder_new.h:1044-1091)
+        const uint32_t enc = (first >> 1) & 0x1fu, fbw = v2_width(enc);
+        uint8_t len = static_cast<uint8_t>((((first & 1u) << 8) | r.byte()) + 1u);
+        uint64_t base = uvarint(r) & M;
+        const int64_t u = static_cast<int64_t>(uvarint(r));
+        const uint64_t bd = static_cast<uint64_t>((u >> 1) ^ -(u & 1)) & M;  // arithmetic shift (:990)
+        o.put(base);
+        base = (base + bd) & M;
+        o.put(base);
+        len = static_cast<uint8_t>(len - 2);
+        const bool plus = bd > 0;  // multiplier = base_delta > 0 ? 1 : -1 on the unsigned type (:1057)
+        if (enc != 0) {
+          HeaderBits b{0, 0};
+          while (len-- > 0) {
+            const uint64_t d = b.read(r, fbw) & M;
+            base = (plus ? base + d : base - d) & M;
+            o.put(base);
+          }
+        } else {
+          while (len-- > 0) {
+            base = (base + bd) & M;
+            o.put(base);
+          }
+        }
+      } break;
+      default: {  // PATCHED_BASE (decoder_new.h:1092-1183)
+        const uint32_t fbw = v2_width((first >> 1) & 0x1fu);
+        uint8_t len = static_cast<uint8_t>((((first & 1u) << 8) | r.byte()) + 1u);
+        const uint32_t third = r.byte(), fourth = r.byte();
+        uint32_t bw = ((third >> 5) & 7u) + 1u;
+        const uint32_t pw = v2_width(third & 0x1fu), pgw = ((fourth >> 5) & 7u) + 1u;
+        uint32_t pll = fourth & 0x1fu;
+        const uint64_t pmask = pw >= 32 ? 0xFFFFFFFFull : ((1ull << pw) - 1ull);  // 32-bit mask (:1103)
+        const uint32_t base_out = o.n;
+        uint64_t base = 0;
+        while (bw-- > 0) base |= shl64(r.byte(), bw * 8u);
+        HeaderBits b{0, 0};
+        while (len-- > 0) o.put((b.read(r, fbw) + base) & M);
+        if (pw + pgw > 64) return CODAG_ECORRUPT;
+        const uint32_t cfb = v2_closest(pw + pgw);
+        b = HeaderBits{0, 0};
+        uint64_t gap = 0;
+        while (pll-- > 0) {
+          const uint64_t ent = b.read(r, cfb);
+          gap += shr64(ent, pw);
+          const uint64_t idx = base_out + gap;
+          if (r.bad || idx >= o.n || o.over) return CODAG_ECORRUPT;
+          const uint64_t patch = shl64((ent & pmask) & M, fbw) & M;
+          const uint64_t v = o.get(static_cast<uint32_t>(idx));
+          o.set(static_cast<uint32_t>(idx), ((((v - base) & M) | patch) + base) & M);
+        }
+      } break;
+    }
+    if (r.bad || o.over) return CODAG_ECORRUPT;
+  }
+  return CODAG_OK;
+}
+
+// values of substream t whose elements fall below `store`
+__device__ __forceinline__ uint32_t needed(uint32_t t, uint32_t ru, uint32_t store) {
+  const uint32_t grp = 32u * ru, g = store / grp, rem = store % grp;
+  const uint32_t lo = t * ru;
+  return g * ru + (rem > lo ? (rem - lo < ru ? rem - lo : ru) : 0u);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) k_rlev2_transposed(const uint8_t* __restrict__ comp, uint64_t comp_bytes,
+                                                          const uint64_t* __restrict__ blk_off,
+                                                          const uint64_t* __restrict__ col_len, uint64_t n_chunks,
+                                                          uint64_t chunk_bytes, uint32_t ru, uint8_t* __restrict__ out,
+                                                          uint64_t out_bytes, int32_t* __restrict__ status,
+                                                          uint32_t max_words) {
+  extern __shared__ uint32_t tabs[];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint64_t c = static_cast<uint64_t>(blockIdx.x) * (blockDim.x >> 5) + warp;
+  if (c >= n_chunks) return;
+  uint32_t* mask = tabs + warp * 2u * max_words;
+  uint32_t* start = mask + max_words;
+  const uint64_t len64 = col_len[32 * c + lane];
+  const uint32_t words = static_cast<uint32_t>(len64 < (1ull << 34) ? (len64 + 3) / 4 : 0xffffffffu);
+  const uint32_t maxw = __reduce_max_sync(FULL, words);
+  const uint64_t total = 4ull * __reduce_add_sync(FULL, words);
+  const uint64_t off = blk_off[c];
+  int st = CODAG_OK;
+  if (maxw > max_words || (off & 3u) || off > comp_bytes || total > comp_bytes - off) st = CODAG_ECORRUPT;
+  const uint64_t base_e = c * (chunk_bytes / sizeof(T));
+  const uint64_t store_b = c * chunk_bytes < out_bytes ? (out_bytes - c * chunk_bytes < chunk_bytes
+                                                             ? out_bytes - c * chunk_bytes : chunk_bytes) : 0;
+  const uint32_t store = static_cast<uint32_t>(store_b / sizeof(T));
+  if (st == CODAG_OK) {
+    uint32_t run = 0;
+    for (uint32_t w = 0; w < maxw; w++) {  // row w: substreams with a word w, words before it
+      const uint32_t m = __ballot_sync(FULL, words > w);
+      if (lane == 0) {
+        mask[w] = m;
+        start[w] = run;
+      }
+      run += __popc(m);
+    }
+    __syncwarp();
+    LaneReader r{reinterpret_cast<const uint32_t*>(comp + off), mask, start, (1u << lane) - 1u,
+                 static_cast<uint32_t>(len64), 0, 0xffffffffu, 0, false};
+    LaneOut<T> o{reinterpret_cast<T*>(out) + base_e, lane, ru,
+                 static_cast<uint32_t>(chunk_bytes / sizeof(T) / 32), store, 0, false};
+    int s = decode_substream<T>(r, o);
+    if (s == CODAG_OK && o.n < needed(lane, ru, store)) s = CODAG_ECORRUPT;
+    st = __reduce_max_sync(FULL, static_cast<uint32_t>(s));
+  }
+  if (status && lane == 0) status[c] = st;
+}
+
+bool valid_elem(int e) { return e == 1 || e == 2 || e == 4 || e == 8; }
+
+template <typename T>
+codag_status launch(const uint8_t* comp, uint64_t comp_bytes, const uint64_t* blk_off, const uint64_t* col_len,
+                    uint64_t n, uint64_t chunk, uint32_t ru, uint8_t* out, uint64_t out_bytes, int32_t* status,
+                    cudaStream_t s) {
+  // a substream is at most about twice its share of the chunk (the encoders' bound), in words
+  const uint32_t max_words = static_cast<uint32_t>((chunk / 32 * 2 + 1024) / 4);
+  constexpr uint32_t kWarps = 4;
+  const uint32_t smem = kWarps * 2u * max_words * 4u;
+  auto kern = k_rlev2_transposed<T>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) != cudaSuccess)
+    return CODAG_ECUDA;
+  const uint64_t grid = (n + kWarps - 1) / kWarps;
+  if (grid > 0x7fffffffull) return CODAG_EINVAL;
+  kern<<<static_cast<unsigned>(grid), 32 * kWarps, smem, s>>>(comp, comp_bytes, blk_off, col_len, n, chunk, ru, out,
+                                                              out_bytes, status, max_words);
+  return cudaGetLastError() == cudaSuccess ? CODAG_OK : CODAG_ECUDA;
+}
+
+}  // namespace
+
+extern "C" codag_status codag_decompress_rlev2_transposed(const uint8_t* d_comp, uint64_t comp_bytes,
+                                                          const uint64_t* d_blk_off, const uint64_t* d_col_len,
+                                                          uint64_t n_chunks, uint64_t chunk_bytes, int elem_bytes,
+                                                          int read_unit, uint8_t* d_out, uint64_t out_bytes,
+                                                          int32_t* d_chunk_status, codag_stream_t stream) {
+  if (!d_comp || !d_blk_off || !d_col_len || (!d_out && out_bytes) || !valid_elem(elem_bytes) || read_unit <= 0 ||
+      chunk_bytes == 0 || chunk_bytes >= (1ull << 31) ||
+      chunk_bytes % (32ull * static_cast<uint64_t>(read_unit) * static_cast<uint64_t>(elem_bytes)) ||
+      (reinterpret_cast<uintptr_t>(d_out) % elem_bytes) || (reinterpret_cast<uintptr_t>(d_comp) & 3u))
+    return CODAG_EINVAL;
+  if (n_chunks == 0) return CODAG_OK;
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const uint32_t ru = static_cast<uint32_t>(read_unit);
+  switch (elem_bytes) {
+    case 8: return launch<uint64_t>(d_comp, comp_bytes, d_blk_off, d_col_len, n_chunks, chunk_bytes, ru, d_out, out_bytes, d_chunk_status, s);
+    case 4: return launch<uint32_t>(d_comp, comp_bytes, d_blk_off, d_col_len, n_chunks, chunk_bytes, ru, d_out, out_bytes, d_chunk_status, s);
+    case 2: return launch<uint16_t>(d_comp, comp_bytes, d_blk_off, d_col_len, n_chunks, chunk_bytes, ru, d_out, out_bytes, d_chunk_status, s);
+    default: return launch<uint8_t>(d_comp, comp_bytes, d_blk_off, d_col_len, n_chunks, chunk_bytes, ru, d_out, out_bytes, d_chunk_status, s);
+  }
+}

@@ -24,7 +24,7 @@ RLEV1, RLEV2, DEFLATE = 0, 1, 2
 # every symbol declared in include/codag.h (libcodag_b200.so)
 EXPORTS = (
     "codag_decompress_rlev1", "codag_decompress_rlev2", "codag_decompress_deflate", "codag_workspace_bytes",
-    "codag_decompress_rlev2_noalloc",
+    "codag_decompress_rlev2_noalloc", "codag_decompress_rlev2_transposed",
     "codag_set_tune", "codag_get_tune", "codag_set_wait_limit", "codag_selftest_wait_timeout",
     "codag_batch_plan", "codag_batch_run", "codag_batch_destroy", "codag_batch_launch",
     "codag_compress_chunks", "codag_compress_bound", "codag_compress_workspace_bytes",
@@ -33,7 +33,7 @@ EXPORTS = (
 # every symbol declared in include/codag_format.h (libcodag_fmt.so)
 FMT_EXPORTS = (
     "codag_hbuf_free", "codag_encode_rlev1", "codag_encode_rlev2", "codag_encode_deflate", "codag_encode_one",
-    "codag_encode_set", "codag_encode_cudf_deflate", "codag_cudf_deflate_layout",
+    "codag_encode_set", "codag_encode_cudf_deflate", "codag_cudf_deflate_layout", "codag_encode_rlev2_transposed",
     "codag_gen_rlev1_column", "codag_gen_rlev2_column", "codag_gen_text",
 )
 
@@ -84,6 +84,8 @@ def lib() -> C.CDLL:
     L.codag_decompress_rlev2_noalloc.argtypes = [vp, u64, vp, vp, u64, u64, C.c_int, vp, u64, vp, vp]
     L.codag_decompress_rlev2_noalloc.restype = i32
     L.codag_decompress_deflate.argtypes = [vp, u64, vp, u64, u64, C.c_int, vp, u64, vp, vp]
+    L.codag_decompress_rlev2_transposed.argtypes = [vp, u64, vp, vp, u64, u64, C.c_int, C.c_int, vp, u64, vp, vp]
+    L.codag_decompress_rlev2_transposed.restype = i32
     L.codag_decompress_deflate.restype = i32
     L.codag_set_tune.argtypes = [C.c_int, C.POINTER(Tune)]
     L.codag_get_tune.argtypes = [C.c_int, C.POINTER(Tune)]
@@ -127,9 +129,12 @@ def fmt_lib() -> C.CDLL:
     L.codag_encode_one.argtypes = [C.c_int, vp, u64, C.c_int, C.c_int, C.POINTER(HBuf)]
     L.codag_encode_set.argtypes = [vp, vp, vp, vp, vp, u64, C.c_int, vp, C.POINTER(HBuf), C.POINTER(u64)]
     L.codag_encode_cudf_deflate.argtypes = [vp, u64, u64, C.c_int, C.POINTER(HBuf)]
+    L.codag_encode_rlev2_transposed.argtypes = [vp, u64, u64, C.c_int, C.c_int, C.POINTER(HBuf), C.POINTER(HBuf),
+                                                C.POINTER(HBuf)]
     L.codag_cudf_deflate_layout.argtypes = [vp, u64, C.POINTER(u64), C.POINTER(u64), C.POINTER(u64), vp]
     for name in ("codag_encode_rlev1", "codag_encode_rlev2", "codag_encode_deflate", "codag_encode_one",
-                 "codag_encode_set", "codag_encode_cudf_deflate", "codag_cudf_deflate_layout"):
+                 "codag_encode_set", "codag_encode_cudf_deflate", "codag_cudf_deflate_layout",
+                 "codag_encode_rlev2_transposed"):
         getattr(L, name).restype = i32
     for name in ("codag_gen_rlev1_column", "codag_gen_rlev2_column"):
         getattr(L, name).argtypes = [u64, u64, C.c_int, vp]
@@ -190,6 +195,15 @@ def encode_deflate(data: np.ndarray, chunk_bytes: int = 131072, level: int = 6, 
                                                             int(zlib_wrapper), int(require_no_stored),
                                                             C.byref(b1), C.byref(b2), C.byref(b3)))
     return _take(b1), _take(b2, np.uint64), _take(b3, np.uint64)
+
+
+def encode_rlev2_transposed(data: np.ndarray, chunk_bytes: int = 131072, elem_bytes: int = 8, read_unit: int = 4):
+    """CODAG's transposed RLE v2 layout (codag_encode_rlev2_transposed): (comp, blk_off[n+1], col_len[n*32])."""
+    raw = np.ascontiguousarray(data).view(np.uint8).reshape(-1)
+    comp, off, ln = HBuf(), HBuf(), HBuf()
+    check("codag_encode_rlev2_transposed", fmt_lib().codag_encode_rlev2_transposed(
+        _ptr(raw), raw.nbytes, chunk_bytes, elem_bytes, read_unit, C.byref(comp), C.byref(off), C.byref(ln)))
+    return _take(comp), _take(off, np.uint64), _take(ln, np.uint64)
 
 
 def encode_cudf_deflate(data: np.ndarray, chunk_bytes: int = 65536, level: int = 9) -> np.ndarray:

@@ -74,6 +74,23 @@ codag_status codag_decompress_rlev2(const uint8_t *d_comp, uint64_t comp_bytes,
                                     void *d_workspace, uint64_t workspace_bytes,
                                     codag_stream_t stream);
 
+/*
+ * ORC RLE v2 in CODAG's transposed layout: each chunk is 32 substreams interleaved in 4-byte
+ * words (codag_encode_rlev2_transposed of codag_format.h writes it).  Replaces
+ * rlev2::decompress_gpu<READ_UNIT,...> (include/rlev2/decoder_trans.h:10-56, the inflate kernel of
+ * decoder_new.h:1193-1230 with decoder_warp :375-632).
+ *   d_blk_off   n_chunks offsets of the chunks' regions (4-byte aligned; 128 in CODAG's layout)
+ *   d_col_len   n_chunks*32 exact substream lengths
+ *   read_unit   values per substream turn (the READ_UNIT template argument); chunk_bytes must
+ *               be a multiple of 32 * read_unit * elem_bytes
+ * Output as for the other decoders: chunk i at d_out + i*chunk_bytes, stored up to out_bytes.
+ */
+codag_status codag_decompress_rlev2_transposed(const uint8_t *d_comp, uint64_t comp_bytes,
+                                               const uint64_t *d_blk_off, const uint64_t *d_col_len,
+                                               uint64_t n_chunks, uint64_t chunk_bytes, int elem_bytes,
+                                               int read_unit, uint8_t *d_out, uint64_t out_bytes,
+                                               int32_t *d_chunk_status, codag_stream_t stream);
+
 /* Workspace bytes the two-pass RLE decode of n_chunks chunks uses (0 for Deflate). */
 uint64_t codag_workspace_bytes(int codec, uint64_t n_chunks);
 

@@ -42,6 +42,15 @@ codag_status codag_encode_rlev2(const uint8_t *in, uint64_t in_bytes, uint64_t c
 codag_status codag_encode_deflate(const uint8_t *in, uint64_t in_bytes, uint64_t chunk_bytes,
                                   int level, int zlib_wrapper, int require_no_stored,
                                   codag_hbuf *comp, codag_hbuf *blk_offset, codag_hbuf *col_len);
+/* CODAG's transposed RLE v2 layout (include/rlev2/encoder_trans.h:8-182 and 359-391,
+ * rlev2::compress_gpu_transpose :411-480): n = ceil(in_bytes/chunk_bytes) chunks, each split into
+ * 32 substreams (substream t = values t*read_unit + k*32*read_unit + j, j < read_unit) encoded on
+ * their own and interleaved in 4-byte words; blk_off has n+1 entries (128-byte aligned regions,
+ * blk_off[n] = in_bytes), col_len n*32 exact substream lengths.  chunk_bytes must be a multiple
+ * of 32 * read_unit * elem_bytes. */
+codag_status codag_encode_rlev2_transposed(const uint8_t *in, uint64_t in_bytes, uint64_t chunk_bytes,
+                                           int elem_bytes, int read_unit, codag_hbuf *comp,
+                                           codag_hbuf *blk_off, codag_hbuf *col_len);
 /* CODAG's cuDF-comparison layout (rapids_compressor.py:222-275, read by
  * include/base_deflate.h:20-130): file = [u64 chunk_bytes][u64 n][u64 size_i x n] then the n
  * zlib-wrapped streams back to back, one per chunk of the input zero padded to a multiple of

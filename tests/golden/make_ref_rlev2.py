@@ -65,6 +65,17 @@ def mixed_column(n: int, elem: int, seed: int, zero_run: int = 100, rand_bits: i
         return np.concatenate(parts)[:n].astype(DT[elem])
 
 
+def transposed_cases():
+    """CODAG's transposed layout: (elem, read_unit, column); partial last chunks included."""
+    from codag_b200 import native
+    return {
+        "c2_u64_ru4": (8, 4, native.gen_rlev2_column(2 * CH // 8 + 333, 211, 8).view(np.uint64)),
+        "mix_u32_ru8": (4, 8, mixed_column(2 * CH // 4 - 9, 4, 212)),
+        "mix_u16_ru2": (2, 2, mixed_column(CH // 2 + 17, 2, 213)),
+        "mix_u8_ru1": (1, 1, mixed_column(CH + 5, 1, 214)),
+    }
+
+
 def cases():
     from codag_b200 import native
     # name: column (the product's seeded generator of the RLE v2 benchmark column, and the
@@ -112,6 +123,16 @@ def main() -> None:
                                 comp=comp, blk_off=blk_off, col_len=col_len, kinds=kinds)
             print(name, "elem", elem, "chunks", col_len.size, "bytes", comp.size, "chunks read as written",
                   len(clean), "headers", dict(zip(KINDS, kinds.tolist())))
+        for name, (elem, ru, col) in transposed_cases().items():
+            col.tofile(t / "col.bin")
+            subprocess.run([str(exe), "transposed", str(elem), str(ru), str(t / "col.bin"), str(t / "r")], check=True,
+                           capture_output=True)
+            comp = np.fromfile(t / "r_comp.bin", np.uint8)
+            blk_off = np.fromfile(t / "r_blk_off.bin", np.uint64)
+            col_len = np.fromfile(t / "r_col_len.bin", np.uint64)
+            np.savez_compressed(out / f"ref_rlev2t_{name}.npz", src=col.view(np.uint8), elem=np.int64(elem),
+                                read_unit=np.int64(ru), comp=comp, blk_off=blk_off, col_len=col_len)
+            print("transposed", name, "elem", elem, "read_unit", ru, "chunks", blk_off.size - 1, "bytes", comp.size)
 
 
 if __name__ == "__main__":

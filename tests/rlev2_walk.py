@@ -70,3 +70,32 @@ def walk(stream) -> dict:
             out["delta_packed" if enc else "delta_fixed"] += 1
             p = q + ((ln - 2) * WIDTH[enc] + 7) // 8 if enc else q
     return out
+
+
+def detranspose(region, lens) -> list:
+    """The 32 substreams of one chunk of CODAG's transposed RLE v2 layout: the region interleaves
+    them in 4-byte words, row w holding word w of every substream longer than 4w, in substream
+    order (include/rlev2/encoder_trans.h:359-391)."""
+    r = bytes(region)
+    words = [(int(x) + 3) // 4 for x in lens]
+    subs = [bytearray() for _ in lens]
+    p = 0
+    for w in range(max(words, default=0)):
+        for t, n in enumerate(words):
+            if n > w:
+                subs[t] += r[p:p + 4]
+                p += 4
+    return [bytes(s[:int(x)]) for s, x in zip(subs, lens)]
+
+
+def interleave_values(subvals, ru: int, elem: int) -> bytes:
+    """Chunk bytes from the 32 substreams' decoded values (bytes, elem-byte little-endian
+    values): value k of substream t is element t*ru + (k//ru)*32*ru + k%ru."""
+    import numpy as np
+    dt = {1: np.uint8, 2: np.uint16, 4: np.uint32, 8: np.uint64}[elem]
+    per = len(subvals[0]) // elem
+    out = np.zeros(32 * per, dt)
+    k = np.arange(per)
+    for t, sv in enumerate(subvals):
+        out[t * ru + (k // ru) * 32 * ru + k % ru] = np.frombuffer(sv, dt)
+    return out.tobytes()
