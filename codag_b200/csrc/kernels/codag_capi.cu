@@ -196,6 +196,69 @@ __global__ void __launch_bounds__(256) k_inflate_plain(const uint8_t* __restrict
   if (status && lane == 0) status[chunk] = st;
 }
 
+// One CTA of two warps per Deflate chunk (codag_tune.cta_per_chunk): warp 2p decodes the symbols
+// of chunk p of the CTA into tokens, warp 2p+1 expands them (decode_deflate.cuh, TokenPipe /
+// expand_tokens); pair p synchronises on named barrier p+1.
+template <int NSLOT, int LB>
+struct InflatePairLayout {
+  using W = typename InflateWinOf<LB>::T;
+  static constexpr uint32_t kIn = 0;
+  static constexpr uint32_t kBar = kIn + NSLOT * kSlotBytes;
+  static constexpr uint32_t kScratch = align_up(kBar + NSLOT * 8, 16);
+  static constexpr uint32_t kOut = align_up(kScratch + sizeof(InflateScratch<LB>), 128);
+  static constexpr uint32_t kTok = kOut + W::kBytes;
+  static constexpr uint32_t kPerPair = align_up(kTok + sizeof(TokenShared), 128);
+};
+
+template <int NSLOT, int LB>
+__global__ void __launch_bounds__(256) k_inflate_cta(const uint8_t* __restrict__ comp, uint64_t comp_bytes,
+                                                     const uint64_t* __restrict__ blk_off, uint64_t n_chunks,
+                                                     uint64_t chunk_bytes, uint32_t wrapper, uint8_t* __restrict__ out,
+                                                     uint64_t out_bytes, int32_t* __restrict__ status,
+                                                     uint64_t wait_cycles) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  using L = InflatePairLayout<NSLOT, LB>;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, pair = warp >> 1;
+  const uint64_t chunk = static_cast<uint64_t>(blockIdx.x) * (blockDim.x >> 6) + pair;
+  uint8_t* base = smem + pair * L::kPerPair;
+  TokenShared* sh = reinterpret_cast<TokenShared*>(base + L::kTok);
+  if ((warp & 1u) == 0 && lane == 0) sh->done = 0;
+  __syncthreads();
+  if (chunk >= n_chunks) return;  // both warps of the pair leave together
+  const uint32_t bar = pair + 1u;
+  const uint64_t off = blk_off[chunk], next = blk_off[chunk + 1];
+  const uint64_t cbase = chunk * chunk_bytes;
+  const bool bad = next < off || !stream_in_bounds(off, next - off, comp_bytes);
+  if ((warp & 1u) == 0) {  // decoder
+    InRing<NSLOT> in;
+    in.buf = base + L::kIn;
+    in.sbuf = smem_u32(in.buf);
+    in.bar = reinterpret_cast<uint64_t*>(base + L::kBar);
+    in.phase = 0;
+    in.wait_cycles = wait_cycles;
+    in.lane = lane;
+    init_ring_barriers<NSLOT>(in.bar, lane);
+    auto& sc = *reinterpret_cast<InflateScratch<LB>*>(base + L::kScratch);
+    TokenPipe pipe{sh, bar, 0, 0, lane};
+    int st = CODAG_ECORRUPT;
+    if (!bad) {
+      in.begin(comp + off, static_cast<uint32_t>(next - off));
+      NullOut none;
+      st = decode_deflate_chunk<NSLOT, LB>(in, none, sc, chunk_bytes, wrapper, &pipe);
+    }
+    pipe.finish(st);
+  } else {  // expander
+    typename L::W o;
+    o.buf = base + L::kOut;
+    o.sbuf = smem_u32(o.buf);
+    o.lane = lane;
+    o.begin(out + cbase, store_bytes(cbase, chunk_bytes, out_bytes));
+    const int est = expand_tokens(sh, bar, o, lane);
+    const int dst = sh->status;
+    if (status && lane == 0) status[chunk] = dst != CODAG_OK ? dst : est;
+  }
+}
+
 // ---------------------------------------------------------------------------------------
 // batched persistent kernel
 // ---------------------------------------------------------------------------------------
@@ -541,6 +604,23 @@ codag_status launch_inflate(const codag_tune& t, const uint8_t* comp, uint64_t c
   return finish_launch();
 }
 
+template <int NSLOT, int LB>
+codag_status launch_inflate_cta(const codag_tune& t, const uint8_t* comp, uint64_t comp_bytes, const uint64_t* blk_off,
+                                uint64_t n, uint64_t chunk_bytes, int wrapper, uint8_t* out, uint64_t out_bytes,
+                                int32_t* status, cudaStream_t s) {
+  using L = InflatePairLayout<NSLOT, LB>;
+  const uint32_t pairs = static_cast<uint32_t>(t.warps_per_cta) / 2u;
+  const uint32_t smem = L::kPerPair * pairs;
+  auto kern = k_inflate_cta<NSLOT, LB>;
+  if (allow_smem(kern, smem) != cudaSuccess) return CODAG_ECUDA;
+  const uint64_t grid = (n + pairs - 1) / pairs;
+  if (grid > 0x7fffffffull) return CODAG_EINVAL;
+  kern<<<static_cast<unsigned>(grid), 64 * pairs, smem, s>>>(comp, comp_bytes, blk_off, n, chunk_bytes,
+                                                             static_cast<uint32_t>(wrapper), out, out_bytes, status,
+                                                             wait_of());
+  return finish_launch();
+}
+
 template <int CODEC>
 codag_status dispatch_rle(const uint8_t* comp, uint64_t comp_bytes, const uint64_t* blk_off, const uint64_t* col_len,
                           uint64_t n, uint64_t chunk_bytes, int e, uint8_t* out, uint64_t out_bytes, int32_t* status,
@@ -650,8 +730,12 @@ extern "C" codag_status codag_decompress_deflate(const uint8_t* d_comp, uint64_t
   if (n_chunks == 0) return CODAG_OK;
   const codag_tune t = tune_of(CODAG_CODEC_DEFLATE);
   const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-#define CODAG_INF(NS, LB) \
-  return launch_inflate<NS, LB>(t, d_comp, comp_bytes, d_blk_off, n_chunks, chunk_bytes, wrapper_bytes, d_out, out_bytes, d_chunk_status, s)
+#define CODAG_INF(NS, LB)                                                                                               \
+  return t.cta_per_chunk                                                                                                \
+             ? launch_inflate_cta<NS, LB>(t, d_comp, comp_bytes, d_blk_off, n_chunks, chunk_bytes, wrapper_bytes, d_out, \
+                                          out_bytes, d_chunk_status, s)                                                 \
+             : launch_inflate<NS, LB>(t, d_comp, comp_bytes, d_blk_off, n_chunks, chunk_bytes, wrapper_bytes, d_out,     \
+                                      out_bytes, d_chunk_status, s)
   if (t.ring_slots == 2) {
     if (t.lut_bits == 9) CODAG_INF(2, 9);
     if (t.lut_bits == 10) CODAG_INF(2, 10);
@@ -675,7 +759,9 @@ extern "C" codag_status codag_set_tune(int codec, const codag_tune* tune) {
   // an RLE v2 header with its data spans up to 2060 bytes; it must fit the window of
   // (slots - 1) KiB ahead of the read position
   if (codec != CODAG_CODEC_DEFLATE && tune->ring_slots < 4) return CODAG_EINVAL;
-  if (tune->cta_per_chunk != 0 && (tune->cta_per_chunk != 1 || codec == CODAG_CODEC_DEFLATE)) return CODAG_EINVAL;
+  if (tune->cta_per_chunk != 0 && tune->cta_per_chunk != 1) return CODAG_EINVAL;
+  // a Deflate chunk per CTA takes a decoder and an expander warp: an even count, up to 4 pairs
+  if (codec == CODAG_CODEC_DEFLATE && tune->cta_per_chunk && (tune->warps_per_cta & 1)) return CODAG_EINVAL;
   std::lock_guard<std::mutex> g(g_mu);
   g_tune[codec] = *tune;
   return CODAG_OK;

@@ -224,9 +224,78 @@ struct BitReader {
   __device__ __forceinline__ uint64_t bitpos() const { return static_cast<uint64_t>(wpos) * 8u - bc; }
 };
 
-template <int NSLOT, int LB, class OUT>
+// ---------------------------------------------------------------------------------------
+// Decoder/expander pairs (one CTA of two warps per chunk)
+// ---------------------------------------------------------------------------------------
+// The decoder warp runs the block and symbol loops below but emits tokens instead of bytes; the
+// expander warp turns the tokens into output through the usual window.  Tokens travel in two
+// shared-memory batches handed over with a named barrier of the pair's 64 threads: after
+// barrier k the decoder fills one batch while the expander drains the other, and each side
+// reaches barrier k+1 only when done with its batch, so neither ever spins.
+// Token: bit 31 set = one or two literals (bits 0-7, 8-15; bit 16 = two); clear = a match,
+// length in bits 0-8 and distance in bits 9-24.
+constexpr uint32_t kTokBatch = 512;
+struct TokenShared {
+  uint32_t tok[2][kTokBatch];
+  uint32_t cnt[2];
+  uint32_t done;
+  int32_t status;
+};
+
+__device__ __forceinline__ void pair_barrier(uint32_t id) {
+  asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory");
+}
+
+struct NoTokens {  // single-warp decode: bytes go straight to the window
+  static constexpr bool kOn = false;
+  __device__ __forceinline__ void literal(uint32_t, uint32_t) {}
+  __device__ __forceinline__ void match(uint32_t, uint32_t) {}
+};
+
+struct TokenPipe {
+  static constexpr bool kOn = true;
+  TokenShared* sh;
+  uint32_t bar, k, n, lane;
+  __device__ __forceinline__ void handoff() {
+    __syncwarp();
+    if (lane == 0) sh->cnt[k] = n;
+    pair_barrier(bar);
+    k ^= 1u;
+    n = 0;
+  }
+  __device__ __forceinline__ void push(uint32_t t) {
+    if (lane == 0) sh->tok[k][n] = t;
+    if (++n == kTokBatch) handoff();
+  }
+  // one literal, or two (second in bits 8-15 when `two`)
+  __device__ __forceinline__ void literal(uint32_t bytes, uint32_t two) { push(0x80000000u | (two << 16) | bytes); }
+  __device__ __forceinline__ void match(uint32_t len, uint32_t dist) { push(len | (dist << 9)); }
+  // the last batch, with the decoder's status
+  __device__ __forceinline__ void finish(int st) {
+    __syncwarp();
+    if (lane == 0) {
+      sh->cnt[k] = n;
+      sh->status = st;
+      sh->done = 1;
+    }
+    pair_barrier(bar);
+  }
+};
+
+// Output stand-in for the decoder warp of a pair, which writes no bytes itself.
+struct NullOut {
+  static constexpr uint32_t kBytes = 4096, kFlush = 1024;
+  uint32_t flushed = 0, store = 0;
+  uint8_t* gdst = nullptr;
+  __device__ __forceinline__ void put8(uint32_t, uint32_t) {}
+  __device__ __forceinline__ uint32_t get8(uint32_t) const { return 0; }
+  __device__ __forceinline__ void flush_to(uint32_t) {}
+  __device__ __forceinline__ void finish(uint32_t) {}
+};
+
+template <int NSLOT, int LB, class OUT, class TOK = NoTokens>
 __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<LB>& sc, uint64_t chunk_bytes,
-                                    uint32_t wrapper) {
+                                    uint32_t wrapper, TOK* tok = nullptr) {
   // Before each symbol fewer than kFlush bytes of the window are unflushed; what is written
   // until the next flush (a match of up to 258 bytes, a piece of a stored block) must not wrap
   // onto them.
@@ -292,7 +361,14 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<
         if (!in.release(p)) { st = CODAG_ETIMEOUT; break; }
         st = in.ensure(p + piece);
         if (st) break;
-        for (uint32_t t = lane; t < piece; t += 32) out.put8(op + t, in.rd8(p + t));
+        if constexpr (TOK::kOn) {  // two bytes per literal token
+          for (uint32_t t = 0; t < piece; t += 2) {
+            const uint32_t two = t + 1 < piece ? 1u : 0u;
+            tok->literal(in.rd8(p + t) | (two ? in.rd8(p + t + 1) << 8 : 0u), two);
+          }
+        } else {
+          for (uint32_t t = lane; t < piece; t += 32) out.put8(op + t, in.rd8(p + t));
+        }
         op += piece;
         p += piece;
         left -= piece;
@@ -393,6 +469,11 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<
       if ((e & kKindMask) == kKindLitBits) {  // one literal or a pair
         const uint32_t pair = (e >> 11) & 1u;
         br.drop(e & 31u);
+        if constexpr (TOK::kOn) {
+          tok->literal(((e >> 16) & 0xffu) | ((e >> 16) & 0xff00u), pair);
+          op += 1u + pair;
+          continue;
+        }
         if (lane <= pair) out.put8(op + lane, lane ? e >> 24 : (e >> 16) & 0xffu);
         op += 1u + pair;
         if (op - out.flushed >= OUT::kFlush) CODAG_FLUSH();
@@ -403,6 +484,11 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<
         if (!e) { st = CODAG_ECORRUPT; break; }
         if ((e & kKindMask) == kKindLitBits) {
           br.drop(e & 31u);
+          if constexpr (TOK::kOn) {
+            tok->literal((e >> 16) & 0xffu, 0u);
+            op++;
+            continue;
+          }
           if (lane == 0) out.put8(op, (e >> 16) & 0xffu);
           op++;
           if (op - out.flushed >= OUT::kFlush) CODAG_FLUSH();
@@ -432,6 +518,11 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<
       const uint32_t dist = (d >> 16) + bfe32(static_cast<uint32_t>(br.bb), dn, dt - dn);
       br.drop(dt);
       if (dist > op || op + len > cap) { st = CODAG_ECORRUPT; break; }
+      if constexpr (TOK::kOn) {
+        tok->match(len, dist);
+        op += len;
+        continue;
+      }
       const uint32_t src = op - dist;
       if (dist + len <= OUT::kBytes) {  // source still in the shared-memory window
         if (src < pend_end) CODAG_COMPLETE();
@@ -481,6 +572,81 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<
   if (st == CODAG_OK && (op < out.store || op > cap || br.bitpos() > static_cast<uint64_t>(in.hi) * 8u))
     st = CODAG_ECORRUPT;
   return st;
+}
+
+// Expander warp of a pair: drains the decoder's token batches into `out` (the window and far
+// copies of decode_deflate_chunk).  Returns CODAG_OK or CODAG_ECORRUPT (fewer bytes than the
+// stored part); the decoder's status arrives in sh->status.
+template <class OUT>
+__device__ int expand_tokens(TokenShared* sh, uint32_t bar, OUT& out, uint32_t lane) {
+  static_assert(OUT::kBytes - OUT::kFlush >= 258, "window too small for a match");
+  uint32_t op = 0, k = 0;
+  uint32_t pend_op = 0, pend_len = 0, pend_end = 0, pend_val = 0;
+#define CODAG_COMPLETE()                                     \
+  if (pend_len) {                                            \
+    if (lane < pend_len) out.put8(pend_op + lane, pend_val); \
+    pend_len = 0;                                            \
+    pend_end = 0;                                            \
+  }
+  for (;;) {
+    pair_barrier(bar);
+    const uint32_t cnt = sh->cnt[k], done = sh->done;
+    const uint32_t s_tok = smem_u32(sh->tok[k]);
+    for (uint32_t i = 0; i < cnt; i++) {
+      const uint32_t t = ld_s32(s_tok + 4u * i);
+      if (t >> 31) {  // literals
+        const uint32_t two = (t >> 16) & 1u;
+        if (lane <= two) out.put8(op + lane, lane ? (t >> 8) & 0xffu : t & 0xffu);
+        op += 1u + two;
+      } else {
+        const uint32_t len = t & 0x1ffu, dist = (t >> 9) & 0xffffu;
+        const uint32_t src = op - dist;
+        if (dist + len <= OUT::kBytes) {  // source still in the shared-memory window
+          if (src < pend_end) CODAG_COMPLETE();
+          __syncwarp();
+          if (dist >= len) {
+            for (uint32_t q = lane; q < len; q += 32) out.put8(op + q, out.get8(src + q));
+          } else {
+            uint32_t r = lane % dist;
+            const uint32_t step = 32u % dist;
+            for (uint32_t q = lane; q < len; q += 32) {
+              out.put8(op + q, out.get8(src + r));
+              r += step;
+              if (r >= dist) r -= dist;
+            }
+          }
+        } else if (len <= 32) {  // flushed already: load now, write into the window later
+          CODAG_COMPLETE();
+          pend_val = (lane < len && src + lane < out.store) ? static_cast<uint32_t>(out.gdst[src + lane]) : 0u;
+          pend_op = op;
+          pend_len = len;
+          pend_end = op + len;
+        } else {
+          CODAG_COMPLETE();
+          const uint32_t r0 = dist >= len ? lane : lane % dist;
+          const uint32_t step = dist >= len ? 32u : 32u % dist;
+          uint32_t r = r0;
+          for (uint32_t q = lane; q < len; q += 32) {
+            const uint32_t sp = src + r;
+            out.put8(op + q, sp < out.store ? out.gdst[sp] : 0u);
+            r += step;
+            if (dist < len && r >= dist) r -= dist;
+          }
+        }
+        op += len;
+      }
+      if (op - out.flushed >= OUT::kFlush) {
+        CODAG_COMPLETE();
+        out.flush_to(op);
+      }
+    }
+    k ^= 1u;
+    if (done) break;
+  }
+  CODAG_COMPLETE();
+#undef CODAG_COMPLETE
+  out.finish(op);
+  return op < out.store ? CODAG_ECORRUPT : CODAG_OK;
 }
 
 }  // namespace codag_dev

@@ -27,7 +27,9 @@ CACHE = Path(os.environ.get("CODAG_TUNE_CACHE", Path(__file__).resolve().parent 
 def candidates(codec: int):
     warps = (1, 2, 4, 8)
     if codec == native.DEFLATE:
-        return list(itertools.product(warps, (2, 4, 8), (9, 10, 11)))
+        # one warp per chunk, or a decoder and an expander warp per chunk (1, 2 or 4 pairs per CTA)
+        return (list(itertools.product(warps, (2, 4, 8), (9, 10, 11), (0,))) +
+                list(itertools.product((2, 4, 8), (4,), (9, 10), (1,))))
     # one warp per chunk, or one CTA of 4 or 8 warps per chunk
     return list(itertools.product(warps, (4, 8), (10,), (0,))) + [(4, 4, 10, 1), (8, 4, 10, 1)]
 

@@ -175,12 +175,14 @@ codag_status codag_compress_rlev2(const uint8_t *d_in, uint64_t in_bytes, uint64
  * RLE v2 header with its data spans up to 2060 bytes); lut_bits the primary Huffman table width
  * (Deflate only: 9, 10 or 11), which also sizes the shared-memory history window of the
  * Deflate call (9: 1 KiB, so more warps fit per SM, for many chunks; 10 and 11: 2 KiB, fewer
- * instructions per chunk, for few chunks).  cta_per_chunk (RLE only, 0 or 1) switches the RLE calls
- * without a workspace to one CTA of warps_per_cta warps per chunk: the CTA stages the
- * chunk's stream in shared memory, one warp walks its headers and all warps expand them,
- * which shortens the decode of a single chunk (few chunks, e.g. an 8 MiB column) at the cost
- * of throughput on many chunks; it applies when the output and out_bytes are element
- * aligned.  Values outside the supported sets return CODAG_EINVAL. */
+ * instructions per chunk, for few chunks).  cta_per_chunk (0 or 1) shortens the decode of a single
+ * chunk (few chunks, e.g. an 8 MiB column, or large files) at the cost of throughput on many:
+ * for the RLE calls without a workspace it runs one CTA of warps_per_cta warps per chunk (the
+ * CTA stages the chunk's stream in shared memory, one warp walks its headers and all warps
+ * expand them; applies when the output and out_bytes are element aligned); for Deflate a
+ * chunk takes two warps, one decoding its symbols into tokens and one expanding them into
+ * bytes, warps_per_cta/2 chunks per CTA (warps_per_cta even).  Values outside the supported
+ * sets return CODAG_EINVAL. */
 typedef struct {
     int32_t warps_per_cta;
     int32_t ring_slots;

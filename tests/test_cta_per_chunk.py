@@ -24,12 +24,18 @@ def cta_mode(codec, warps):
         native.set_tune(codec, old.warps_per_cta, old.ring_slots, old.lut_bits, old.cta_per_chunk)
 
 
-def test_tune_accepts_cta_mode_for_rle_only(native):
+def test_tune_accepts_cta_mode(native):
     with cta_mode(RLEV2, 8):
         assert native.get_tune(RLEV2).cta_per_chunk == 1
     assert native.get_tune(RLEV2).cta_per_chunk == 0
-    with pytest.raises(native.CodagError):
-        native.set_tune(native.DEFLATE, 2, 2, 9, 1)
+    old = native.get_tune(native.DEFLATE)
+    try:  # Deflate: a decoder and an expander warp per chunk, so an even warp count
+        native.set_tune(native.DEFLATE, 4, 2, 9, 1)
+        assert native.get_tune(native.DEFLATE).cta_per_chunk == 1
+        with pytest.raises(native.CodagError):
+            native.set_tune(native.DEFLATE, 3, 2, 9, 1)
+    finally:
+        native.set_tune(native.DEFLATE, old.warps_per_cta, old.ring_slots, old.lut_bits, old.cta_per_chunk)
     with pytest.raises(native.CodagError):
         native.set_tune(RLEV1, 8, 4, 10, 2)
 

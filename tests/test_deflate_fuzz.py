@@ -74,9 +74,11 @@ def test_oracle_decodes_adversarial_chunks(oracle):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("cta", [(0, None), (1, 2), (1, 8)], ids=["warp", "cta_1pair", "cta_4pairs"])
 @pytest.mark.parametrize("lut", [9, 10, 11])  # 9 bits: 1 KiB window; 10 and 11: 2 KiB
 @pytest.mark.parametrize("seed", [2, 3])
-def test_gpu_decodes_adversarial_chunks(cuda, native, seed, lut):
+def test_gpu_decodes_adversarial_chunks(cuda, native, seed, lut, cta):
+    """One warp per chunk, or a decoder and an expander warp per chunk (cta_per_chunk)."""
     from codag_b200 import api
     comp, rel, src = _streams(seed, 36)
     n = rel.size - 1
@@ -85,7 +87,7 @@ def test_gpu_decodes_adversarial_chunks(cuda, native, seed, lut):
     out = cuda.full((n * CH + 64,), 0xA5, dtype=cuda.uint8, device="cuda")
     st = cuda.full((n,), -1, dtype=cuda.int32, device="cuda")
     old = native.get_tune(native.DEFLATE)
-    native.set_tune(native.DEFLATE, old.warps_per_cta, old.ring_slots, lut)
+    native.set_tune(native.DEFLATE, cta[1] or old.warps_per_cta, old.ring_slots, lut, cta[0])
     try:
         api.decompress_deflate(d_comp, d_rel, CH, out, 2, n * CH, st)
         cuda.cuda.synchronize()
@@ -119,3 +121,39 @@ def test_batch_kernel_decodes_adversarial_chunks(cuda, native):
     for i in range(n):
         a = int(cs.descs[i]["out_off"])
         assert np.array_equal(o[a:a + CH], src[i * CH:(i + 1) * CH]), i
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", [5, 6])
+def test_cta_per_chunk_matches_one_warp_on_damaged_streams(cuda, native, seed):
+    """Streams with bytes flipped: the decoder/expander pair reports the same status per chunk
+    as the one-warp decoder, and the same bytes wherever that status is OK."""
+    from codag_b200 import api
+    comp, rel, src = _streams(seed, 24)
+    rng = np.random.default_rng(seed)
+    n = rel.size - 1
+    bad = comp.copy()
+    for i in range(n):  # flip a few bytes inside most chunks
+        lo, hi = int(rel[i]) + 2, int(rel[i + 1])
+        if i % 3 and hi > lo:
+            for p in rng.integers(lo, hi, 3):
+                bad[p] ^= np.uint8(rng.integers(1, 256))
+    d_comp = cuda.from_numpy(bad).to("cuda")
+    d_rel = cuda.from_numpy(rel.view(np.int64)).to("cuda")
+    old = native.get_tune(native.DEFLATE)
+    res = []
+    try:
+        for warps, cta in ((old.warps_per_cta, 0), (4, 1)):
+            native.set_tune(native.DEFLATE, warps, old.ring_slots, old.lut_bits, cta)
+            out = cuda.zeros(n * CH, dtype=cuda.uint8, device="cuda")
+            st = cuda.full((n,), -1, dtype=cuda.int32, device="cuda")
+            api.decompress_deflate(d_comp, d_rel, CH, out, 2, n * CH, st)
+            cuda.cuda.synchronize()
+            res.append((st.cpu().numpy(), out.cpu().numpy()))
+    finally:
+        native.set_tune(native.DEFLATE, old.warps_per_cta, old.ring_slots, old.lut_bits, old.cta_per_chunk)
+    (s1, o1), (s2, o2) = res
+    assert np.array_equal(s1, s2)
+    assert (s1 != 0).any() and (s1 == 0).any()
+    for i in np.flatnonzero(s1 == 0):
+        assert np.array_equal(o1[i * CH:(i + 1) * CH], o2[i * CH:(i + 1) * CH]), i
