@@ -126,10 +126,7 @@ def main(args, rank: int, world: int, local: int):
             shape = tuple(hit)
         else:
             res = {}
-            for cand in tuning.candidates(2):
-                if cand[1] < 4 or cand[3]:  # the batch kernel: one warp per chunk, RLE-sized rings
-                    continue
-                cand = cand[:3]
+            for cand in tuning.batch_candidates():
                 p = api.BatchPlan(ms.descs, *cand)
                 res[cand] = tuning.time_call(lambda: p.run(d_comp, d_out, d_st, use_graph=False), reps=2)
                 p.close()

@@ -265,12 +265,17 @@ __global__ void __launch_bounds__(256) k_inflate_cta(const uint8_t* __restrict__
 // The Deflate window is the plain kernel's (InflateWinOf<LB>), small enough for many resident
 // warps; RLE values go straight to global memory (element by element when the output is
 // element aligned, byte by byte otherwise), so no RLE header needs the window.
+// With n_pair > 0 (a plan made with cta_per_chunk), the first n_pair entries of the work order
+// are large Deflate files taken by pairs of warps: warp 2p of a CTA decodes the symbols into
+// tokens, warp 2p+1 expands them, the tokens passing through the expander's idle input ring
+// (TokenShared), each job fenced by named barrier p+1; the pair counter is queue[1].  When those
+// run out, every warp pulls the remaining entries on its own from queue[0].
 template <int NSLOT, int LB>
 __global__ void __launch_bounds__(256) k_batch(const codag_chunk_desc* __restrict__ descs,
                                                const uint32_t* __restrict__ order, uint64_t n,
                                                uint32_t* __restrict__ queue, const uint8_t* __restrict__ comp,
                                                uint64_t comp_bytes, uint8_t* __restrict__ out, uint64_t out_bytes,
-                                               int32_t* __restrict__ status, uint64_t wait_cycles) {
+                                               int32_t* __restrict__ status, uint64_t wait_cycles, uint32_t n_pair) {
   extern __shared__ __align__(128) uint8_t smem[];
   using W = typename InflateWinOf<LB>::T;
   using L = InflateLayout<NSLOT, LB, W>;
@@ -293,6 +298,45 @@ __global__ void __launch_bounds__(256) k_batch(const codag_chunk_desc* __restric
   ob.lane = lane;
   auto& sc = *reinterpret_cast<InflateScratch<LB>*>(base + L::kScratch);
   init_ring_barriers<NSLOT>(in.bar, lane);
+
+  if (n_pair) {  // large Deflate files, one pair of warps each
+    const uint32_t bar = (warp >> 1) + 1u;
+    const bool decoder = (warp & 1u) == 0;
+    TokenShared* sh = reinterpret_cast<TokenShared*>(smem + (warp | 1u) * L::kPerWarp + L::kIn);
+    for (;;) {
+      if (decoder && lane == 0) {
+        sh->job = atomicAdd(queue + 1, 1u);
+        sh->done = 0;
+      }
+      pair_barrier(bar);
+      const uint32_t k = sh->job;
+      if (k >= n_pair) break;
+      const uint32_t i = order[k];
+      const codag_chunk_desc d = descs[i];
+      const bool ok = d.codec == CODAG_CODEC_DEFLATE && d.out_off <= out_bytes && d.out_len <= out_bytes - d.out_off &&
+                      stream_in_bounds(d.comp_off, d.comp_len, comp_bytes);
+      if (decoder) {
+        TokenPipe pipe{sh, bar, 0, 0, lane};
+        int st = CODAG_ECORRUPT;
+        if (ok) {
+          in.begin(comp + d.comp_off, d.comp_len);
+          NullOut none;
+          st = decode_deflate_chunk<NSLOT, LB>(in, none, sc, d.out_len, d.wrapper_bytes, &pipe);
+        }
+        pipe.finish(st);
+      } else {
+        o.begin(out + d.out_off, ok ? d.out_len : 0);
+        const int est = expand_tokens(sh, bar, o, lane);
+        const int dst = sh->status;
+        if (status && lane == 0) status[i] = dst != CODAG_OK ? dst : est;
+      }
+      const bool timed_out = sh->status == CODAG_ETIMEOUT;
+      pair_barrier(bar);  // the expander has read this job's status before the next job begins
+      if (timed_out) return;  // ring state unknown: both warps stop
+    }
+    order += n_pair;
+    n -= n_pair;
+  }
 
   for (;;) {
     uint32_t k = 0;
@@ -791,6 +835,7 @@ extern "C" codag_status codag_selftest_wait_timeout(int32_t* d_status, codag_str
 // ---------------------------------------------------------------------------------------
 struct codag_plan {
   uint64_t n = 0;
+  uint32_t n_pair = 0;  // leading entries of the order decoded by warp pairs (large Deflate files)
   codag_tune tune{};
   codag_chunk_desc* d_descs = nullptr;
   uint32_t* d_order = nullptr;
@@ -832,7 +877,7 @@ void batch_launch(codag_plan* p, const uint8_t* comp, uint64_t comp_bytes, uint8
   using L = BatchLayout<NSLOT, LB>;
   const uint32_t smem = L::kPerWarp * p->tune.warps_per_cta;
   k_batch<NSLOT, LB><<<p->grid, 32 * p->tune.warps_per_cta, smem, s>>>(
-      p->d_descs, p->d_order, p->n, p->d_queue, comp, comp_bytes, out, out_bytes, status, wait_of());
+      p->d_descs, p->d_order, p->n, p->d_queue, comp, comp_bytes, out, out_bytes, status, wait_of(), p->n_pair);
 }
 
 #define CODAG_BATCH_SWITCH(FN, ...)                      \
@@ -867,12 +912,15 @@ codag_status batch_setup_any(codag_plan* p) {
 
 void batch_enqueue(codag_plan* p, const uint8_t* comp, uint64_t comp_bytes, uint8_t* out, uint64_t out_bytes,
                    int32_t* status, cudaStream_t s) {
-  cudaMemsetAsync(p->d_queue, 0, sizeof(uint32_t), s);
+  cudaMemsetAsync(p->d_queue, 0, (p->n_pair ? 2 : 1) * sizeof(uint32_t), s);
   CODAG_BATCH_SWITCH(batch_launch, p, comp, comp_bytes, out, out_bytes, status, s);
 }
 
 // work estimate used to order the queue: compressed bytes, Deflate weighted by its
 // per-byte decode cost relative to the RLE codecs
+// Deflate files at least this long go to warp pairs in a plan made with cta_per_chunk
+constexpr uint32_t kPairMinBytes = 256u << 10;
+
 uint64_t chunk_cost(const codag_chunk_desc& d) {
   return d.codec == CODAG_CODEC_DEFLATE ? 8ull * d.comp_len + d.out_len : static_cast<uint64_t>(d.comp_len) + d.out_len / 4;
 }
@@ -884,7 +932,8 @@ extern "C" codag_status codag_batch_plan(const codag_chunk_desc* h_descs, uint64
   if (!h_descs || !plan || n == 0 || n > 0xffffffffull) return CODAG_EINVAL;
   codag_tune t = tune ? *tune : tune_of(CODAG_CODEC_DEFLATE);
   if (!valid_warps(t.warps_per_cta) || !valid_slots(t.ring_slots) || !valid_lut(t.lut_bits)) return CODAG_EINVAL;
-  if (t.ring_slots < 4) t.ring_slots = 4;  // mixed batches include RLE chunks
+  if (t.cta_per_chunk != 0 && (t.cta_per_chunk != 1 || (t.warps_per_cta & 1))) return CODAG_EINVAL;
+  if (t.ring_slots < 4) t.ring_slots = 4;  // mixed batches include RLE chunks (and the token batches need 4 KiB)
   for (uint64_t i = 0; i < n; i++) {
     const codag_chunk_desc& d = h_descs[i];
     if (d.codec > CODAG_CODEC_DEFLATE) return CODAG_EINVAL;
@@ -896,11 +945,19 @@ extern "C" codag_status codag_batch_plan(const codag_chunk_desc* h_descs, uint64
   p->tune = t;
   std::vector<uint32_t> order(n);
   for (uint64_t i = 0; i < n; i++) order[i] = static_cast<uint32_t>(i);
-  std::stable_sort(order.begin(), order.end(),
-                   [&](uint32_t a, uint32_t b) { return chunk_cost(h_descs[a]) > chunk_cost(h_descs[b]); });
+  // with cta_per_chunk, Deflate files of at least kPairMinBytes go first, to warp pairs
+  auto paired = [&](uint32_t i) {
+    return t.cta_per_chunk && h_descs[i].codec == CODAG_CODEC_DEFLATE && h_descs[i].out_len >= kPairMinBytes;
+  };
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+    const bool pa = paired(a), pb = paired(b);
+    if (pa != pb) return pa;
+    return chunk_cost(h_descs[a]) > chunk_cost(h_descs[b]);
+  });
+  for (uint64_t i = 0; i < n && paired(order[i]); i++) p->n_pair++;
   if (cudaMalloc(&p->d_descs, n * sizeof(codag_chunk_desc)) != cudaSuccess ||
       cudaMalloc(&p->d_order, n * sizeof(uint32_t)) != cudaSuccess ||
-      cudaMalloc(&p->d_queue, sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&p->d_queue, 2 * sizeof(uint32_t)) != cudaSuccess ||
       cudaMemcpy(p->d_descs, h_descs, n * sizeof(codag_chunk_desc), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(p->d_order, order.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess) {
     codag_batch_destroy(p);

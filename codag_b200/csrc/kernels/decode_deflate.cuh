@@ -234,13 +234,17 @@ struct BitReader {
 // reaches barrier k+1 only when done with its batch, so neither ever spins.
 // Token: bit 31 set = one or two literals (bits 0-7, 8-15; bit 16 = two); clear = a match,
 // length in bits 0-8 and distance in bits 9-24.
-constexpr uint32_t kTokBatch = 512;
+// 496 tokens a batch: the two batches and their counters fit in 4 KiB (the batched kernel keeps
+// them in the expander warp's idle input ring)
+constexpr uint32_t kTokBatch = 496;
 struct TokenShared {
   uint32_t tok[2][kTokBatch];
   uint32_t cnt[2];
   uint32_t done;
   int32_t status;
+  uint32_t job;  // batched kernel: the pair's current job
 };
+static_assert(sizeof(TokenShared) <= 4096, "token batches must fit a 4 KiB ring");
 
 __device__ __forceinline__ void pair_barrier(uint32_t id) {
   asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory");

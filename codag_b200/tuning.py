@@ -34,6 +34,14 @@ def candidates(codec: int):
     return list(itertools.product(warps, (4, 8), (10,), (0,))) + [(4, 4, 10, 1), (8, 4, 10, 1)]
 
 
+def batch_candidates():
+    """Launch shapes of the batched kernel: (warps_per_cta, ring_slots, lut_bits, cta_per_chunk);
+    RLE files need rings of at least 4 slots; with cta_per_chunk the large Deflate files go to
+    warp pairs, so the warp count is even."""
+    return (list(itertools.product((1, 2, 4, 8), (4, 8), (9, 10, 11), (0,))) +
+            list(itertools.product((2, 4, 8), (4,), (9, 10, 11), (1,))))
+
+
 def _key(codec: int, tag: str) -> str:
     return f"{torch.cuda.get_device_name()}|codec{codec}|{tag}"
 

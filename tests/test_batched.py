@@ -143,3 +143,59 @@ def test_batch_host_pipeline_matches_source(cuda, small_set, steps):
             assert np.array_equal(h.numpy(), ms.expected())
     finally:
         pipe.close()
+
+
+@pytest.fixture(scope="module")
+def large_set(native):
+    return batched.make_mixed_set(160, seed=101, max_bytes=1 << 20, source_bytes=16 << 20)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("use_graph", [False, True])
+@pytest.mark.parametrize("shape", [(2, 4, 9, 1), (4, 4, 10, 1), (8, 4, 11, 1)])
+def test_batched_warp_pairs_match_source(cuda, large_set, shape, use_graph):
+    """Plans made with cta_per_chunk: Deflate files of 256 KiB or more decoded by warp pairs
+    (symbol decoder and byte expander), everything else by single warps."""
+    from codag_b200 import api
+    ms = large_set
+    big = (ms.codecs == 2) & (ms.in_len >= (256 << 10))
+    assert big.sum() >= 4
+    plan = api.BatchPlan(ms.descs, *shape)
+    try:
+        out = cuda.zeros(ms.out_bytes, dtype=cuda.uint8, device="cuda")
+        st = cuda.full((ms.n,), -1, dtype=cuda.int32, device="cuda")
+        for _ in range(2):
+            out.zero_()
+            plan.run(cuda.from_numpy(ms.comp).to("cuda"), out, st, use_graph=use_graph)
+            cuda.cuda.synchronize()
+            assert int((st != 0).sum().item()) == 0
+            assert np.array_equal(out.cpu().numpy(), ms.expected())
+    finally:
+        plan.close()
+
+
+@pytest.mark.gpu
+def test_batched_warp_pairs_report_damage_like_single_warps(cuda, large_set):
+    from codag_b200 import api
+    ms = large_set
+    comp = ms.comp.copy()
+    rng = np.random.default_rng(3)
+    for i in np.flatnonzero(ms.codecs == 2)[::2]:  # damage every other Deflate file
+        d = ms.descs[i]
+        comp[int(d["comp_off"]) + 2 + rng.integers(0, int(d["comp_len"]) - 2, 4)] ^= 0x5A
+    res = []
+    for shape in ((4, 4, 10, 0), (4, 4, 10, 1)):
+        plan = api.BatchPlan(ms.descs, *shape)
+        try:
+            out = cuda.zeros(ms.out_bytes, dtype=cuda.uint8, device="cuda")
+            st = cuda.full((ms.n,), -1, dtype=cuda.int32, device="cuda")
+            plan.run(cuda.from_numpy(comp).to("cuda"), out, st)
+            cuda.cuda.synchronize()
+            res.append((st.cpu().numpy(), out.cpu().numpy()))
+        finally:
+            plan.close()
+    (s1, o1), (s2, o2) = res
+    assert np.array_equal(s1, s2) and (s1 != 0).any()
+    for i in np.flatnonzero(s1 == 0):
+        a, ln = int(ms.descs[i]["out_off"]), int(ms.in_len[i])
+        assert np.array_equal(o1[a:a + ln], o2[a:a + ln]), i
