@@ -302,15 +302,17 @@ class BatchPlan:
     """codag_batch_plan/run/destroy: one persistent launch over many independent chunks."""
 
     def __init__(self, descs: np.ndarray, warps_per_cta: int | None = None, ring_slots: int | None = None,
-                 lut_bits: int | None = None, cta_per_chunk: int = 0):
+                 lut_bits: int | None = None, cta_per_chunk: int = 0, table_global: int = 0):
         """cta_per_chunk=1 (warps_per_cta even): Deflate files of 256 KiB or more are decoded
-        first, each by a pair of warps (symbol decoder and byte expander)."""
+        first, each by a pair of warps (symbol decoder and byte expander).  table_global=1: the
+        Huffman lookup tables in global memory (read through L1) instead of shared memory."""
         descs = np.ascontiguousarray(descs, dtype=native.CHUNK_DESC_DTYPE)
         self.n = descs.size
         tune = None
         if warps_per_cta is not None:
             d = native.get_tune(native.DEFLATE)
-            tune = native.Tune(warps_per_cta, ring_slots or d.ring_slots, lut_bits or d.lut_bits, cta_per_chunk)
+            tune = native.Tune(warps_per_cta, ring_slots or d.ring_slots, lut_bits or d.lut_bits, cta_per_chunk,
+                               table_global)
         p = C.c_void_p()
         check("codag_batch_plan", native.lib().codag_batch_plan(descs.ctypes.data, self.n,
                                                                 C.byref(tune) if tune is not None else None,

@@ -26,7 +26,7 @@ FMT_LIB = PKG / "libcodag_fmt.so"
 EXE = REPO / "build" / "exe" / "src"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fopenmp", "-Xptxas", "-warn-spills"]
+NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++20", "-Xcompiler", "-fPIC,-fopenmp", "-Xptxas", "-warn-spills"]
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fopenmp", "-Wall", "-Wno-unused-function"]
 
 HOST_SOURCES = sorted((CSRC / "host").glob("*.cpp"))

@@ -61,12 +61,12 @@ struct RleDirectLayout {
   static constexpr uint32_t kPerWarp = align_up(kBar + NSLOT * 8, 128);
 };
 
-template <int NSLOT, int LB, class OUT>
+template <int NSLOT, int LB, class OUT, class SCR = InflateScratch<LB>>
 struct InflateLayout {
   static constexpr uint32_t kIn = 0;
   static constexpr uint32_t kOut = kIn + NSLOT * kSlotBytes;
   static constexpr uint32_t kScratch = kOut + OUT::kBytes;
-  static constexpr uint32_t kBar = align_up(kScratch + sizeof(InflateScratch<LB>), 16);
+  static constexpr uint32_t kBar = align_up(kScratch + sizeof(SCR), 16);
   static constexpr uint32_t kPerWarp = align_up(kBar + NSLOT * 8, 128);
 };
 
@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(256) k_inflate_plain(const uint8_t* __restrict
   } else {
     in.begin(comp + off, static_cast<uint32_t>(next - off));
     o.begin(out + cbase, store_bytes(cbase, chunk_bytes, out_bytes));
-    st = decode_deflate_chunk<NSLOT, LB>(in, o, sc, chunk_bytes, wrapper);
+    st = decode_deflate_chunk<NSLOT, LB>(in, o, sc, sc.lit_lut, sc.dist_lut, chunk_bytes, wrapper);
   }
   if (status && lane == 0) status[chunk] = st;
 }
@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(256) k_inflate_cta(const uint8_t* __restrict__
     if (!bad) {
       in.begin(comp + off, static_cast<uint32_t>(next - off));
       NullOut none;
-      st = decode_deflate_chunk<NSLOT, LB>(in, none, sc, chunk_bytes, wrapper, &pipe);
+      st = decode_deflate_chunk<NSLOT, LB>(in, none, sc, sc.lit_lut, sc.dist_lut, chunk_bytes, wrapper, &pipe);
     }
     pipe.finish(st);
   } else {  // expander
@@ -270,15 +270,19 @@ __global__ void __launch_bounds__(256) k_inflate_cta(const uint8_t* __restrict__
 // tokens, warp 2p+1 expands them, the tokens passing through the expander's idle input ring
 // (TokenShared), each job fenced by named barrier p+1; the pair counter is queue[1].  When those
 // run out, every warp pulls the remaining entries on its own from queue[0].
-template <int NSLOT, int LB>
+// GT: the Huffman lookup tables live in global memory (gtab, kLutEntries<LB> words per warp of
+// the grid, read through L1) instead of shared memory.
+template <int NSLOT, int LB, bool GT>
 __global__ void __launch_bounds__(256) k_batch(const codag_chunk_desc* __restrict__ descs,
                                                const uint32_t* __restrict__ order, uint64_t n,
                                                uint32_t* __restrict__ queue, const uint8_t* __restrict__ comp,
                                                uint64_t comp_bytes, uint8_t* __restrict__ out, uint64_t out_bytes,
-                                               int32_t* __restrict__ status, uint64_t wait_cycles, uint32_t n_pair) {
+                                               int32_t* __restrict__ status, uint64_t wait_cycles, uint32_t n_pair,
+                                               uint32_t* __restrict__ gtab) {
   extern __shared__ __align__(128) uint8_t smem[];
   using W = typename InflateWinOf<LB>::T;
-  using L = InflateLayout<NSLOT, LB, W>;
+  using SCR = std::conditional_t<GT, InflateCodes, InflateScratch<LB>>;
+  using L = InflateLayout<NSLOT, LB, W, SCR>;
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   uint8_t* base = smem + warp * L::kPerWarp;
   InRing<NSLOT> in;
@@ -296,7 +300,15 @@ __global__ void __launch_bounds__(256) k_batch(const codag_chunk_desc* __restric
   od.lane = lane;
   ByteOut ob;
   ob.lane = lane;
-  auto& sc = *reinterpret_cast<InflateScratch<LB>*>(base + L::kScratch);
+  auto& sc = *reinterpret_cast<SCR*>(base + L::kScratch);
+  uint32_t *lit_lut, *dist_lut;
+  if constexpr (GT) {
+    lit_lut = gtab + (static_cast<uint64_t>(blockIdx.x) * (blockDim.x >> 5) + warp) * kLutEntries<LB>;
+    dist_lut = lit_lut + (1u << LB);
+  } else {
+    lit_lut = sc.lit_lut;
+    dist_lut = sc.dist_lut;
+  }
   init_ring_barriers<NSLOT>(in.bar, lane);
 
   if (n_pair) {  // large Deflate files, one pair of warps each
@@ -321,7 +333,8 @@ __global__ void __launch_bounds__(256) k_batch(const codag_chunk_desc* __restric
         if (ok) {
           in.begin(comp + d.comp_off, d.comp_len);
           NullOut none;
-          st = decode_deflate_chunk<NSLOT, LB>(in, none, sc, d.out_len, d.wrapper_bytes, &pipe);
+          st = decode_deflate_chunk<NSLOT, LB, NullOut, TokenPipe, GT>(in, none, sc, lit_lut, dist_lut, d.out_len,
+                                                                      d.wrapper_bytes, &pipe);
         }
         pipe.finish(st);
       } else {
@@ -353,7 +366,8 @@ __global__ void __launch_bounds__(256) k_batch(const codag_chunk_desc* __restric
       in.begin(comp + d.comp_off, d.comp_len);
       if (d.codec == CODAG_CODEC_DEFLATE) {
         o.begin(out + d.out_off, d.out_len);
-        st = decode_deflate_chunk<NSLOT, LB>(in, o, sc, d.out_len, d.wrapper_bytes);
+        st = decode_deflate_chunk<NSLOT, LB, typename InflateWinOf<LB>::T, NoTokens, GT>(
+            in, o, sc, lit_lut, dist_lut, d.out_len, d.wrapper_bytes);
       } else if (d.codec == CODAG_CODEC_RLEV1 || d.codec == CODAG_CODEC_RLEV2) {
         const uint32_t e = d.elem_bytes;
         if (valid_elem_dev(e) && (reinterpret_cast<uintptr_t>(out + d.out_off) % e) == 0 && d.out_len % e == 0) {
@@ -535,7 +549,7 @@ __global__ void k_selftest_timeout(int32_t* status, uint64_t wait_cycles) {
 // host side
 // ---------------------------------------------------------------------------------------
 std::mutex g_mu;
-codag_tune g_tune[3] = {{8, 4, 10, 0}, {8, 4, 10, 0}, {2, 2, 9, 0}};
+codag_tune g_tune[3] = {{8, 4, 10, 0, 0}, {8, 4, 10, 0, 0}, {2, 2, 9, 0, 0}};
 uint64_t g_wait_cycles = 2000000000ull;  // about one second at 2 GHz
 
 bool valid_slots(int s) { return s == 2 || s == 4 || s == 8; }
@@ -804,6 +818,7 @@ extern "C" codag_status codag_set_tune(int codec, const codag_tune* tune) {
   // (slots - 1) KiB ahead of the read position
   if (codec != CODAG_CODEC_DEFLATE && tune->ring_slots < 4) return CODAG_EINVAL;
   if (tune->cta_per_chunk != 0 && tune->cta_per_chunk != 1) return CODAG_EINVAL;
+  if (tune->table_global != 0) return CODAG_EINVAL;  // per-file calls: tables in shared memory (no workspace)
   // a Deflate chunk per CTA takes a decoder and an expander warp: an even count, up to 4 pairs
   if (codec == CODAG_CODEC_DEFLATE && tune->cta_per_chunk && (tune->warps_per_cta & 1)) return CODAG_EINVAL;
   std::lock_guard<std::mutex> g(g_mu);
@@ -840,6 +855,7 @@ struct codag_plan {
   codag_chunk_desc* d_descs = nullptr;
   uint32_t* d_order = nullptr;
   uint32_t* d_queue = nullptr;
+  uint32_t* d_tab = nullptr;  // Huffman lookup tables of every warp (tune.table_global)
   int grid = 0;
   // captured graph and the arguments it was captured with
   cudaGraphExec_t exec = nullptr;
@@ -851,14 +867,15 @@ struct codag_plan {
 
 namespace {
 
-template <int NSLOT, int LB>
-using BatchLayout = InflateLayout<NSLOT, LB, typename InflateWinOf<LB>::T>;
+template <int NSLOT, int LB, bool GT>
+using BatchLayout = InflateLayout<NSLOT, LB, typename InflateWinOf<LB>::T,
+                                  std::conditional_t<GT, InflateCodes, InflateScratch<LB>>>;
 
-template <int NSLOT, int LB>
+template <int NSLOT, int LB, bool GT>
 codag_status batch_setup(codag_plan* p) {
-  using L = BatchLayout<NSLOT, LB>;
+  using L = BatchLayout<NSLOT, LB, GT>;
   const uint32_t smem = L::kPerWarp * p->tune.warps_per_cta;
-  auto kern = k_batch<NSLOT, LB>;
+  auto kern = k_batch<NSLOT, LB, GT>;
   if (allow_smem(kern, smem) != cudaSuccess) return CODAG_ECUDA;
   int dev = 0, sms = 0, per_sm = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
@@ -871,49 +888,55 @@ codag_status batch_setup(codag_plan* p) {
   return CODAG_OK;
 }
 
-template <int NSLOT, int LB>
-void batch_launch(codag_plan* p, const uint8_t* comp, uint64_t comp_bytes, uint8_t* out, uint64_t out_bytes,
-                  int32_t* status, cudaStream_t s) {
-  using L = BatchLayout<NSLOT, LB>;
+template <int NSLOT, int LB, bool GT>
+codag_status batch_launch(codag_plan* p, const uint8_t* comp, uint64_t comp_bytes, uint8_t* out, uint64_t out_bytes,
+                          int32_t* status, cudaStream_t s) {
+  using L = BatchLayout<NSLOT, LB, GT>;
   const uint32_t smem = L::kPerWarp * p->tune.warps_per_cta;
-  k_batch<NSLOT, LB><<<p->grid, 32 * p->tune.warps_per_cta, smem, s>>>(
-      p->d_descs, p->d_order, p->n, p->d_queue, comp, comp_bytes, out, out_bytes, status, wait_of(), p->n_pair);
+  k_batch<NSLOT, LB, GT><<<p->grid, 32 * p->tune.warps_per_cta, smem, s>>>(
+      p->d_descs, p->d_order, p->n, p->d_queue, comp, comp_bytes, out, out_bytes, status, wait_of(), p->n_pair,
+      p->d_tab);
+  return CODAG_OK;
 }
 
-#define CODAG_BATCH_SWITCH(FN, ...)                      \
-  switch (p->tune.ring_slots * 100 + p->tune.lut_bits) { \
-    case 209: FN<2, 9>(__VA_ARGS__); break;              \
-    case 210: FN<2, 10>(__VA_ARGS__); break;             \
-    case 211: FN<2, 11>(__VA_ARGS__); break;             \
-    case 409: FN<4, 9>(__VA_ARGS__); break;              \
-    case 410: FN<4, 10>(__VA_ARGS__); break;             \
-    case 411: FN<4, 11>(__VA_ARGS__); break;             \
-    case 809: FN<8, 9>(__VA_ARGS__); break;              \
-    case 810: FN<8, 10>(__VA_ARGS__); break;             \
-    default: FN<8, 11>(__VA_ARGS__); break;              \
+// Calls f.template operator()<NSLOT, LB, GT>() for the plan's launch shape.
+template <class F>
+codag_status batch_dispatch(const codag_tune& t, F&& f) {
+  const int key = t.ring_slots * 100 + t.lut_bits;
+#define CODAG_BATCH_CASE(NS, LB)                                                               \
+  case NS * 100 + LB:                                                                          \
+    return t.table_global ? f.template operator()<NS, LB, true>() : f.template operator()<NS, LB, false>();
+  switch (key) {
+    CODAG_BATCH_CASE(2, 9)
+    CODAG_BATCH_CASE(2, 10)
+    CODAG_BATCH_CASE(2, 11)
+    CODAG_BATCH_CASE(4, 9)
+    CODAG_BATCH_CASE(4, 10)
+    CODAG_BATCH_CASE(4, 11)
+    CODAG_BATCH_CASE(8, 9)
+    CODAG_BATCH_CASE(8, 10)
+    default:
+      return t.table_global ? f.template operator()<8, 11, true>() : f.template operator()<8, 11, false>();
   }
+#undef CODAG_BATCH_CASE
+}
 
 codag_status batch_setup_any(codag_plan* p) {
-  codag_status st = CODAG_OK;
-  auto call = [&](auto fn) { st = fn(p); };
-  switch (p->tune.ring_slots * 100 + p->tune.lut_bits) {
-    case 209: call(batch_setup<2, 9>); break;
-    case 210: call(batch_setup<2, 10>); break;
-    case 211: call(batch_setup<2, 11>); break;
-    case 409: call(batch_setup<4, 9>); break;
-    case 410: call(batch_setup<4, 10>); break;
-    case 411: call(batch_setup<4, 11>); break;
-    case 809: call(batch_setup<8, 9>); break;
-    case 810: call(batch_setup<8, 10>); break;
-    default: call(batch_setup<8, 11>); break;
-  }
-  return st;
+  return batch_dispatch(p->tune, [&]<int NS, int LB, bool GT>() { return batch_setup<NS, LB, GT>(p); });
 }
 
 void batch_enqueue(codag_plan* p, const uint8_t* comp, uint64_t comp_bytes, uint8_t* out, uint64_t out_bytes,
                    int32_t* status, cudaStream_t s) {
   cudaMemsetAsync(p->d_queue, 0, (p->n_pair ? 2 : 1) * sizeof(uint32_t), s);
-  CODAG_BATCH_SWITCH(batch_launch, p, comp, comp_bytes, out, out_bytes, status, s);
+  batch_dispatch(p->tune, [&]<int NS, int LB, bool GT>() {
+    return batch_launch<NS, LB, GT>(p, comp, comp_bytes, out, out_bytes, status, s);
+  });
+}
+
+// lookup-table words of a plan whose tables live in global memory (every warp of the grid)
+uint64_t table_words(const codag_plan* p) {
+  const uint64_t per = p->tune.lut_bits == 9 ? kLutEntries<9> : p->tune.lut_bits == 10 ? kLutEntries<10> : kLutEntries<11>;
+  return static_cast<uint64_t>(p->grid) * p->tune.warps_per_cta * per;
 }
 
 // work estimate used to order the queue: compressed bytes, Deflate weighted by its
@@ -933,6 +956,7 @@ extern "C" codag_status codag_batch_plan(const codag_chunk_desc* h_descs, uint64
   codag_tune t = tune ? *tune : tune_of(CODAG_CODEC_DEFLATE);
   if (!valid_warps(t.warps_per_cta) || !valid_slots(t.ring_slots) || !valid_lut(t.lut_bits)) return CODAG_EINVAL;
   if (t.cta_per_chunk != 0 && (t.cta_per_chunk != 1 || (t.warps_per_cta & 1))) return CODAG_EINVAL;
+  if (t.table_global != 0 && t.table_global != 1) return CODAG_EINVAL;
   if (t.ring_slots < 4) t.ring_slots = 4;  // mixed batches include RLE chunks (and the token batches need 4 KiB)
   for (uint64_t i = 0; i < n; i++) {
     const codag_chunk_desc& d = h_descs[i];
@@ -967,6 +991,10 @@ extern "C" codag_status codag_batch_plan(const codag_chunk_desc* h_descs, uint64
   if (st != CODAG_OK) {
     codag_batch_destroy(p);
     return st;
+  }
+  if (t.table_global && cudaMalloc(&p->d_tab, table_words(p) * sizeof(uint32_t)) != cudaSuccess) {
+    codag_batch_destroy(p);
+    return CODAG_ECUDA;
   }
   *plan = p;
   return CODAG_OK;
@@ -1018,6 +1046,7 @@ extern "C" codag_status codag_batch_destroy(codag_plan* p) {
   if (p->d_descs) cudaFree(p->d_descs);
   if (p->d_order) cudaFree(p->d_order);
   if (p->d_queue) cudaFree(p->d_queue);
+  if (p->d_tab) cudaFree(p->d_tab);
   delete p;
   return CODAG_OK;
 }
@@ -1070,6 +1099,7 @@ extern "C" codag_status codag_batch_launch(const codag_chunk_desc* d_descs, cons
   if (!valid_warps(p.tune.warps_per_cta) || !valid_slots(p.tune.ring_slots) || !valid_lut(p.tune.lut_bits))
     return CODAG_EINVAL;
   if (p.tune.ring_slots < 4) p.tune.ring_slots = 4;  // mixed batches include RLE chunks
+  if (p.tune.table_global) return CODAG_EINVAL;         // no plan, so no global table scratch
   int cap = 0;
   const codag_status st = launch_shape(p.tune, &cap);
   if (st != CODAG_OK) return st;

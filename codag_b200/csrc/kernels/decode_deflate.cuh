@@ -172,11 +172,10 @@ __device__ __forceinline__ uint32_t slow_entry(uint64_t bb, const HuffTable& t, 
   return 0;
 }
 
-// per-warp shared memory of the Deflate decoder
-template <int LB>
-struct InflateScratch {
-  uint32_t lit_lut[1u << LB];
-  uint32_t dist_lut[1u << kDistLB];
+// Per-warp shared memory of the Deflate decoder: the current block's canonical codes, and
+// (InflateScratch) its lookup tables.  The batched kernel can keep the lookup tables in
+// global memory instead (read through L1), which frees 3-9 KiB of shared memory per warp.
+struct InflateCodes {
   uint32_t lit_cnt[16], lit_first[16], lit_index[16];
   uint32_t dist_cnt[16], dist_first[16], dist_index[16];
   uint32_t fill[16];
@@ -184,6 +183,21 @@ struct InflateScratch {
   uint16_t dist_sorted[32];
   uint8_t lens[320];
 };
+template <int LB>
+struct InflateScratch : InflateCodes {
+  uint32_t lit_lut[1u << LB];
+  uint32_t dist_lut[1u << kDistLB];
+};
+// entries of the global-memory tables of one warp
+template <int LB>
+constexpr uint32_t kLutEntries = (1u << LB) + (1u << kDistLB);
+
+// table entry i: a shared-memory table (saddr) or a global one (p)
+template <bool GT>
+__device__ __forceinline__ uint32_t lut_ld(const uint32_t* p, uint32_t saddr, uint32_t i) {
+  if constexpr (GT) return p[i];
+  else return ld_s32(saddr + 4u * i);
+}
 
 template <int NSLOT>
 struct BitReader {
@@ -297,9 +311,10 @@ struct NullOut {
   __device__ __forceinline__ void finish(uint32_t) {}
 };
 
-template <int NSLOT, int LB, class OUT, class TOK = NoTokens>
-__device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<LB>& sc, uint64_t chunk_bytes,
-                                    uint32_t wrapper, TOK* tok = nullptr) {
+// GT: lit_lut / dist_lut are global memory (else shared memory, e.g. InflateScratch's).
+template <int NSLOT, int LB, class OUT, class TOK = NoTokens, bool GT = false>
+__device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateCodes& sc, uint32_t* lit_lut,
+                                    uint32_t* dist_lut, uint64_t chunk_bytes, uint32_t wrapper, TOK* tok = nullptr) {
   // Before each symbol fewer than kFlush bytes of the window are unflushed; what is written
   // until the next flush (a match of up to 258 bytes, a piece of a stored block) must not wrap
   // onto them.
@@ -307,10 +322,10 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<
   constexpr uint32_t kStoredPiece = OUT::kBytes - OUT::kFlush < 1024u ? OUT::kBytes - OUT::kFlush : 1024u;
   const uint32_t lane = in.lane;
   const uint32_t cap = static_cast<uint32_t>(chunk_bytes);
-  const HuffTable lit{sc.lit_lut, sc.lit_sorted, sc.lit_cnt, sc.lit_first, sc.lit_index, LB};
-  const HuffTable dst{sc.dist_lut, sc.dist_sorted, sc.dist_cnt, sc.dist_first, sc.dist_index, kDistLB};
-  const HuffTable cl{sc.dist_lut, sc.dist_sorted, sc.dist_cnt, sc.dist_first, sc.dist_index, kCodeLenLB};
-  const uint32_t s_lit = smem_u32(sc.lit_lut), s_dist = smem_u32(sc.dist_lut);
+  const HuffTable lit{lit_lut, sc.lit_sorted, sc.lit_cnt, sc.lit_first, sc.lit_index, LB};
+  const HuffTable dst{dist_lut, sc.dist_sorted, sc.dist_cnt, sc.dist_first, sc.dist_index, kDistLB};
+  const HuffTable cl{dist_lut, sc.dist_sorted, sc.dist_cnt, sc.dist_first, sc.dist_index, kCodeLenLB};
+  const uint32_t s_lit = GT ? 0u : smem_u32(lit_lut), s_dist = GT ? 0u : smem_u32(dist_lut);
 
   uint32_t op = 0;  // bytes produced (chunks are < 2 GiB)
   int st = CODAG_OK;
@@ -423,7 +438,7 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<
       const uint32_t total = hlit + hdist;
       while (idx < total) {
         CODAG_REFILL();
-        const uint32_t e = ld_s32(s_dist + 4u * static_cast<uint32_t>(br.bb & ((1u << kCodeLenLB) - 1u)));
+        const uint32_t e = lut_ld<GT>(dist_lut, s_dist, static_cast<uint32_t>(br.bb & ((1u << kCodeLenLB) - 1u)));
         if (e & kSlowFlag) { st = CODAG_ECORRUPT; break; }  // code lengths are at most 7 bits
         br.drop(e & 31u);
         const uint32_t sym = e >> 16;
@@ -469,7 +484,7 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<
     // symbol loop (zlib.h:712-805)
     for (;;) {
       CODAG_REFILL();
-      uint32_t e = ld_s32(s_lit + ((static_cast<uint32_t>(br.bb) & ((1u << LB) - 1u)) << 2));
+      uint32_t e = lut_ld<GT>(lit_lut, s_lit, static_cast<uint32_t>(br.bb) & ((1u << LB) - 1u));
       if ((e & kKindMask) == kKindLitBits) {  // one literal or a pair
         const uint32_t pair = (e >> 11) & 1u;
         br.drop(e & 31u);
@@ -512,7 +527,7 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateScratch<
         st = br.refill(in);
         if (st) break;
       }
-      uint32_t d = ld_s32(s_dist + ((static_cast<uint32_t>(br.bb) & ((1u << kDistLB) - 1u)) << 2));
+      uint32_t d = lut_ld<GT>(dist_lut, s_dist, static_cast<uint32_t>(br.bb) & ((1u << kDistLB) - 1u));
       if (d & kSlowFlag) {
         d = slow_entry(br.bb, dst, kAlphaDist);
         if (!d) { st = CODAG_ECORRUPT; break; }

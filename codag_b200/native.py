@@ -50,7 +50,7 @@ class HBuf(C.Structure):
 
 class Tune(C.Structure):
     _fields_ = [("warps_per_cta", C.c_int32), ("ring_slots", C.c_int32), ("lut_bits", C.c_int32),
-                ("cta_per_chunk", C.c_int32)]
+                ("cta_per_chunk", C.c_int32), ("table_global", C.c_int32)]
 
 
 class ChunkDesc(C.Structure):

@@ -188,6 +188,11 @@ typedef struct {
     int32_t ring_slots;
     int32_t lut_bits;
     int32_t cta_per_chunk;
+    int32_t table_global; /* batched plans only (0 or 1): the Huffman lookup tables of every warp in
+                             global memory, read through L1, instead of shared memory; frees
+                             3-9 KiB of shared memory per warp for more resident warps.  The
+                             per-file calls and codag_batch_launch keep them in shared memory
+                             (0; other values give CODAG_EINVAL). */
 } codag_tune;
 
 codag_status codag_set_tune(int codec, const codag_tune *tune);

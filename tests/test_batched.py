@@ -34,8 +34,10 @@ def test_stratified_sample_covers_codecs(small_set):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("use_graph", [False, True])
-@pytest.mark.parametrize("shape", [None, (1, 4, 9), (4, 8, 11), (8, 4, 10)])
+@pytest.mark.parametrize("shape", [None, (1, 4, 9), (4, 8, 11), (8, 4, 10), (2, 4, 9, 0, 1), (8, 8, 11, 0, 1)])
 def test_batched_matches_source(cuda, small_set, shape, use_graph):
+    """Shapes (warps_per_cta, ring_slots, lut_bits[, cta_per_chunk, table_global]); the last two
+    keep the Huffman lookup tables in global memory."""
     from codag_b200 import api
     ms = small_set
     d_comp = cuda.from_numpy(ms.comp).to("cuda")
@@ -152,7 +154,7 @@ def large_set(native):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("use_graph", [False, True])
-@pytest.mark.parametrize("shape", [(2, 4, 9, 1), (4, 4, 10, 1), (8, 4, 11, 1)])
+@pytest.mark.parametrize("shape", [(2, 4, 9, 1), (4, 4, 10, 1), (8, 4, 11, 1), (4, 4, 10, 1, 1)])
 def test_batched_warp_pairs_match_source(cuda, large_set, shape, use_graph):
     """Plans made with cta_per_chunk: Deflate files of 256 KiB or more decoded by warp pairs
     (symbol decoder and byte expander), everything else by single warps."""
@@ -199,3 +201,11 @@ def test_batched_warp_pairs_report_damage_like_single_warps(cuda, large_set):
     for i in np.flatnonzero(s1 == 0):
         a, ln = int(ms.descs[i]["out_off"]), int(ms.in_len[i])
         assert np.array_equal(o1[a:a + ln], o2[a:a + ln]), i
+
+
+def test_table_placement_is_a_plan_option(native):
+    """Global-memory lookup tables need the plan's scratch: the per-file calls refuse them."""
+    import ctypes as C
+    t = native.Tune(2, 2, 9, 0, 1)
+    assert native.lib().codag_set_tune(native.DEFLATE, C.byref(t)) == native.EINVAL
+    assert native.get_tune(native.DEFLATE).table_global == 0
