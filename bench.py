@@ -54,6 +54,14 @@ WORKLOADS = {
     "deflate": dict(codec=2, n=1 << 30, elem=1, desc="Deflate (zlib level 6), 1 GiB Zipf text, 8192 x 128 KiB chunks"),
 }
 KERNEL_NAMES = {0: "k_rle_plain<.., RLEV1>", 1: "k_rle_plain<.., RLEV2>", 2: "k_inflate_plain"}
+
+
+def _kernel_name(codec: int, t) -> str:
+    if codec != 2:
+        return "k_rle_cta<RLEV1/RLEV2, E>" if t.cta_per_chunk else KERNEL_NAMES[codec]
+    return "k_inflate_cta" if t.cta_per_chunk else KERNEL_NAMES[codec]
+
+
 EXTRA_CONFIGS = ("rlev2", "rlev1", "rlev1x128", "deflate")
 
 
@@ -326,7 +334,7 @@ def measure_codec(workload: str, args, rank: int, world: int, local: int, steps:
         "gpu_launches": steps * (2 if codec != 2 and args.rle_passes == 2 else 1),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": ncu_traffic(workload), "peak_kind": peak_kind,
-                     "kernel": ("k_rle_cta<RLEV1/RLEV2, E>" if codec != 2 and t.cta_per_chunk else KERNEL_NAMES[codec]),
+                     "kernel": _kernel_name(codec, t),
                      "alg_bytes_per_launch": alg_bytes,
                      "note": ("launch = header walk + expansion kernels of one call" if codec != 2 and args.rle_passes == 2
                               else "one kernel"),

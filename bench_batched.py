@@ -20,7 +20,7 @@ import time
 
 import numpy as np
 
-from bench import METRIC
+from bench import METRIC, ncu_traffic
 
 SEED = 20260104
 
@@ -245,8 +245,9 @@ def main(args, rank: int, world: int, local: int):
                        "pinned host buffers"},
         "gpu_launches": args.steps,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
-                     "kernel": "k_batch", "alg_bytes_per_launch": alg, "launch_ms": round(per_launch * 1e3, 4)},
+                     "frac": round(achieved / peak, 4),
+                     "traffic": ncu_traffic("batched") if (args.n_files or 20_000) == 20_000 else None,
+                     "peak_kind": peak_kind, "kernel": "k_batch", "alg_bytes_per_launch": alg, "launch_ms": round(per_launch * 1e3, 4)},
         "cpu_baseline": cpu,
         "clocks": clk,
     }

@@ -303,9 +303,9 @@ class BatchPlan:
 
     def __init__(self, descs: np.ndarray, warps_per_cta: int | None = None, ring_slots: int | None = None,
                  lut_bits: int | None = None, cta_per_chunk: int = 0, table_global: int = 0):
-        """cta_per_chunk=1 (warps_per_cta even): Deflate files of 256 KiB or more are decoded
-        first, each by a pair of warps (symbol decoder and byte expander).  table_global=1: the
-        Huffman lookup tables in global memory (read through L1) instead of shared memory."""
+        """cta_per_chunk=k in 1..4 (warps_per_cta even): Deflate files of k x 256 KiB or more are
+        decoded first, each by a pair of warps (symbol decoder and byte expander).  table_global=1:
+        the Huffman lookup tables in global memory (read through L1) instead of shared memory."""
         descs = np.ascontiguousarray(descs, dtype=native.CHUNK_DESC_DTYPE)
         self.n = descs.size
         tune = None

@@ -941,8 +941,9 @@ uint64_t table_words(const codag_plan* p) {
 
 // work estimate used to order the queue: compressed bytes, Deflate weighted by its
 // per-byte decode cost relative to the RLE codecs
-// Deflate files at least this long go to warp pairs in a plan made with cta_per_chunk
-constexpr uint32_t kPairMinBytes = 256u << 10;
+// In a plan made with cta_per_chunk = k (1..4), Deflate files of at least k x 256 KiB go to
+// warp pairs
+constexpr uint64_t kPairStepBytes = 256u << 10;
 
 uint64_t chunk_cost(const codag_chunk_desc& d) {
   return d.codec == CODAG_CODEC_DEFLATE ? 8ull * d.comp_len + d.out_len : static_cast<uint64_t>(d.comp_len) + d.out_len / 4;
@@ -955,7 +956,7 @@ extern "C" codag_status codag_batch_plan(const codag_chunk_desc* h_descs, uint64
   if (!h_descs || !plan || n == 0 || n > 0xffffffffull) return CODAG_EINVAL;
   codag_tune t = tune ? *tune : tune_of(CODAG_CODEC_DEFLATE);
   if (!valid_warps(t.warps_per_cta) || !valid_slots(t.ring_slots) || !valid_lut(t.lut_bits)) return CODAG_EINVAL;
-  if (t.cta_per_chunk != 0 && (t.cta_per_chunk != 1 || (t.warps_per_cta & 1))) return CODAG_EINVAL;
+  if (t.cta_per_chunk < 0 || t.cta_per_chunk > 4 || (t.cta_per_chunk && (t.warps_per_cta & 1))) return CODAG_EINVAL;
   if (t.table_global != 0 && t.table_global != 1) return CODAG_EINVAL;
   if (t.ring_slots < 4) t.ring_slots = 4;  // mixed batches include RLE chunks (and the token batches need 4 KiB)
   for (uint64_t i = 0; i < n; i++) {
@@ -969,9 +970,10 @@ extern "C" codag_status codag_batch_plan(const codag_chunk_desc* h_descs, uint64
   p->tune = t;
   std::vector<uint32_t> order(n);
   for (uint64_t i = 0; i < n; i++) order[i] = static_cast<uint32_t>(i);
-  // with cta_per_chunk, Deflate files of at least kPairMinBytes go first, to warp pairs
+  // with cta_per_chunk, the Deflate files of at least cta_per_chunk x 256 KiB go first, to warp pairs
+  const uint64_t pair_min = static_cast<uint64_t>(t.cta_per_chunk) * kPairStepBytes;
   auto paired = [&](uint32_t i) {
-    return t.cta_per_chunk && h_descs[i].codec == CODAG_CODEC_DEFLATE && h_descs[i].out_len >= kPairMinBytes;
+    return t.cta_per_chunk && h_descs[i].codec == CODAG_CODEC_DEFLATE && h_descs[i].out_len >= pair_min;
   };
   std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
     const bool pa = paired(a), pb = paired(b);

@@ -36,11 +36,11 @@ def candidates(codec: int):
 
 def batch_candidates():
     """Launch shapes of the batched kernel: (warps_per_cta, ring_slots, lut_bits, cta_per_chunk,
-    table_global).  RLE files need rings of at least 4 slots; with cta_per_chunk the large
-    Deflate files go to warp pairs, so the warp count is even; table_global places the Huffman
-    lookup tables in global memory (through L1) rather than shared memory."""
+    table_global).  RLE files need rings of at least 4 slots; with cta_per_chunk = k the Deflate
+    files of at least k x 256 KiB go to warp pairs (so the warp count is even); table_global
+    places the Huffman lookup tables in global memory (through L1) rather than shared memory."""
     return (list(itertools.product((2, 4, 8), (4, 8), (9, 10, 11), (0,), (0, 1))) +
-            list(itertools.product((4, 8), (4,), (9, 10, 11), (1,), (0, 1))))
+            list(itertools.product((4, 8), (4,), (9, 10, 11), (1, 2, 3), (0,))))
 
 
 def _key(codec: int, tag: str) -> str:

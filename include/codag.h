@@ -226,7 +226,9 @@ typedef struct {
 typedef struct codag_plan codag_plan;
 
 /* Copies the descriptors to the device (the only allocating call), orders the queue and
- * picks the launch shape (tune may be NULL: use the process-wide defaults). */
+ * picks the launch shape (tune may be NULL: use the process-wide defaults).  In a plan,
+ * tune->cta_per_chunk = k (1..4, warps_per_cta even) sends the Deflate chunks of at least
+ * k x 256 KiB to warp pairs (a symbol decoder and a byte expander each), decoded first. */
 codag_status codag_batch_plan(const codag_chunk_desc *h_descs, uint64_t n, const codag_tune *tune,
                               codag_plan **plan);
 /* One persistent launch over all planned chunks; d_status has n entries (may be NULL).

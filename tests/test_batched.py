@@ -154,14 +154,15 @@ def large_set(native):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("use_graph", [False, True])
-@pytest.mark.parametrize("shape", [(2, 4, 9, 1), (4, 4, 10, 1), (8, 4, 11, 1), (4, 4, 10, 1, 1)])
+@pytest.mark.parametrize("shape", [(2, 4, 9, 1), (4, 4, 10, 1), (8, 4, 11, 1), (4, 4, 10, 1, 1), (4, 4, 10, 2),
+                                   (8, 4, 9, 3)])
 def test_batched_warp_pairs_match_source(cuda, large_set, shape, use_graph):
-    """Plans made with cta_per_chunk: Deflate files of 256 KiB or more decoded by warp pairs
-    (symbol decoder and byte expander), everything else by single warps."""
+    """Plans made with cta_per_chunk = k: Deflate files of k x 256 KiB or more decoded by warp
+    pairs (symbol decoder and byte expander), everything else by single warps."""
     from codag_b200 import api
     ms = large_set
-    big = (ms.codecs == 2) & (ms.in_len >= (256 << 10))
-    assert big.sum() >= 4
+    big = (ms.codecs == 2) & (ms.in_len >= shape[3] * (256 << 10))
+    assert big.sum() >= 2
     plan = api.BatchPlan(ms.descs, *shape)
     try:
         out = cuda.zeros(ms.out_bytes, dtype=cuda.uint8, device="cuda")
@@ -201,6 +202,17 @@ def test_batched_warp_pairs_report_damage_like_single_warps(cuda, large_set):
     for i in np.flatnonzero(s1 == 0):
         a, ln = int(ms.descs[i]["out_off"]), int(ms.in_len[i])
         assert np.array_equal(o1[a:a + ln], o2[a:a + ln]), i
+
+
+def test_pair_threshold_range(native, small_set):
+    """cta_per_chunk in a plan: 0..4 (multiples of 256 KiB) with an even warp count; checked
+    before anything touches the device."""
+    import ctypes as C
+    d = np.ascontiguousarray(small_set.descs, dtype=native.CHUNK_DESC_DTYPE)
+    p = C.c_void_p()
+    for shape in ((4, 4, 10, 5), (4, 4, 10, -1), (3, 4, 10, 2)):
+        t = native.Tune(*shape)
+        assert native.lib().codag_batch_plan(d.ctypes.data, d.size, C.byref(t), C.byref(p)) == native.EINVAL, shape
 
 
 def test_table_placement_is_a_plan_option(native):
