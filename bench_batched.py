@@ -210,17 +210,22 @@ def main(args, rank: int, world: int, local: int):
     e2e_h2d, e2e_d2h = pipe.h2d_bytes, pipe.d2h_bytes
     pipe.close()
     del pipe
+    # whole-job bytes: every rank decodes its own seeded set, so sizes differ between ranks
+    job_out, job_h2d, job_d2h = total_out, int(e2e_h2d), int(e2e_d2h)
     if world > 1:
         okt = torch.tensor([0 if ok else 1], dtype=torch.int32, device=dev)
         dist.all_reduce(okt)
         ok = int(okt.item()) == 0
+        jt = torch.tensor([total_out, job_h2d, job_d2h], dtype=torch.int64, device=dev)
+        dist.all_reduce(jt)
+        job_out, job_h2d, job_d2h = (int(x) for x in jt.tolist())
     if rank != 0:
         plan.close()
         return None
 
     peak, peak_kind = peaks()
     achieved = alg / per_launch / 1e9
-    value = world * total_out * args.steps / elapsed / 1e9
+    value = job_out * args.steps / elapsed / 1e9
     pf_gbs = pf_bytes / pf_t / 1e9
     cpu = None
     if world == 1:
@@ -238,9 +243,9 @@ def main(args, rank: int, world: int, local: int):
         "plain_per_file": {"value": round(pf_gbs, 4), "unit": "GB/s", "files_timed": int(sample.size),
                            "bytes_timed": pf_bytes, "seconds": round(pf_t, 4),
                            "how": "one C-ABI call per file, in order on one stream, stratified sample"},
-        "batched_over_plain": round(value / world / pf_gbs, 1),
-        "e2e": {"value": round(world * total_out * e_steps / e2e_t / 1e9, 2), "unit": "GB/s",
-                "h2d_bytes_per_step": int(e2e_h2d), "d2h_bytes_per_step": int(e2e_d2h),
+        "batched_over_plain": round(total_out * args.steps / elapsed / 1e9 / pf_gbs, 1),
+        "e2e": {"value": round(job_out * e_steps / e2e_t / 1e9, 2), "unit": "GB/s",
+                "h2d_bytes_per_step": job_h2d, "d2h_bytes_per_step": job_d2h,
                 "how": f"api.BatchHostPipeline, {e_steps} steps, H2D/launch/D2H of consecutive steps overlapped, "
                        "pinned host buffers"},
         "gpu_launches": args.steps,

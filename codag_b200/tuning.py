@@ -60,8 +60,11 @@ def store_cached(codec: int, tag: str, shape) -> None:
     except (OSError, ValueError):
         data = {}
     data[_key(codec, tag)] = list(shape)
+    # written whole and renamed into place: ranks of one job may store at the same time
+    tmp = CACHE.with_name(f"{CACHE.name}.{os.getpid()}.tmp")
     try:
-        CACHE.write_text(json.dumps(data, indent=1, sort_keys=True))
+        tmp.write_text(json.dumps(data, indent=1, sort_keys=True))
+        os.replace(tmp, CACHE)
     except OSError:
         pass
 
