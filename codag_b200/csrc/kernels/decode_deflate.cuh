@@ -330,6 +330,7 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateCodes& s
   uint32_t op = 0;  // bytes produced (chunks are < 2 GiB)
   int st = CODAG_OK;
   BitReader<NSLOT> br;
+  const uint32_t lit_sh = 16u + 8u * (lane & 1u);  // first literal in bits 16-23, second in 24-31
   bool fixed_ready = false;
 
   if (in.lo + wrapper > in.hi) st = CODAG_ECORRUPT;
@@ -492,11 +493,17 @@ __device__ int decode_deflate_chunk(InRing<NSLOT>& in, OUT& out, InflateCodes& s
           tok->literal(((e >> 16) & 0xffu) | ((e >> 16) & 0xff00u), pair);
           op += 1u + pair;
           continue;
+        } else {
+          // lane 0 stores the literal, lane 1 the second of a pair: one predicated byte store
+          // of the entry shifted by lit_sh, with no branch on the lane
+          const uint32_t a = out.sbuf + ((op + lane) & OUT::kMask);
+          asm volatile("{ .reg .pred p; setp.le.u32 p, %0, %1; @p st.shared.u8 [%2], %3; }" ::"r"(lane), "r"(pair),
+                       "r"(a), "r"(e >> lit_sh)
+                       : "memory");
+          op += 1u + pair;
+          if (op - out.flushed >= OUT::kFlush) CODAG_FLUSH();
+          continue;
         }
-        if (lane <= pair) out.put8(op + lane, lane ? e >> 24 : (e >> 16) & 0xffu);
-        op += 1u + pair;
-        if (op - out.flushed >= OUT::kFlush) CODAG_FLUSH();
-        continue;
       }
       if (e & kSlowFlag) {
         e = slow_entry(br.bb, lit, kAlphaLitLen);

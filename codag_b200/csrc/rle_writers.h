@@ -228,20 +228,19 @@ constexpr int kMaxShortRepeat = 10;
 
 // number of significant bits rounded up to a representable width (find_closes_num_bits)
 CODAG_HD uint8_t closest_width(uint64_t v) {
-  uint8_t c = 0;
-  while (v) {
-    v >>= 1;
-    ++c;
-  }
-  return v2_closest(c);
+  // bits needed for v (0 for 0): a leading-zero count rather than a 64-step shift loop
+#if defined(__CUDA_ARCH__)
+  const uint32_t c = 64u - static_cast<uint32_t>(__clzll(static_cast<long long>(v)));
+#else
+  const uint32_t c = v ? 64u - static_cast<uint32_t>(__builtin_clzll(v)) : 0u;
+#endif
+  return static_cast<uint8_t>(v2_closest(c));
 }
 
 template <class Sink>
 class RleV2Writer {
  public:
-  CODAG_HD explicit RleV2Writer(Sink& out) : out_(out) {
-    for (int i = 0; i < kMaxLiterals; i++) deltas_[i] = 0;
-  }
+  CODAG_HD explicit RleV2Writer(Sink& out) : out_(out) {}
 
   // n values, value i read as get(i) (zero-extended to 64 bits)
   template <class Get>
@@ -277,13 +276,8 @@ class RleV2Writer {
           var_ -= kMinRepeat - 1;
           choose_encoding();
           prev_delta = 0;
-          for (int k = 0; k < kMinRepeat; ++k) {
-            lit_[k] = val;
-            deltas_[k] = 0;
-          }
+          for (int k = 0; k < kMinRepeat; ++k) lit_[k] = val;
           nlit_ = kMinRepeat;
-        } else if (fix_ >= kMinRepeat) {
-          deltas_[0] = 0;
         }
         if (fix_ == kMaxLiterals) choose_encoding();
         continue;
@@ -332,10 +326,15 @@ class RleV2Writer {
  private:
   CODAG_HD void put(uint8_t b) { out_.put(b); }
 
+  // The writer keeps only the pending values (lit_) and the patch list: deltas and base-reduced
+  // values are derived from lit_ where they are read, which keeps a GPU thread's state small
+  // enough for L1.  d(i) below is any such derived sequence.
+
   // histogram of representable widths (compute_bit_width)
-  CODAG_HD static void width_hist(const uint64_t* d, uint32_t n, uint8_t* hist) {
+  template <class D>
+  CODAG_HD static void width_hist(const D& d, uint32_t n, uint8_t* hist) {
     for (int i = 0; i < 32; i++) hist[i] = 0;
-    for (uint32_t i = 0; i < n; ++i) hist[v2_code(closest_width(d[i]))]++;
+    for (uint32_t i = 0; i < n; ++i) hist[v2_code(closest_width(d(i)))]++;
   }
 
   // smallest width covering all but the top (100-p)% of values (compute_percentile_bit_width)
@@ -350,7 +349,8 @@ class RleV2Writer {
   }
 
   // fixed width big-endian packing used by DIRECT and DELTA (write_aligned_ints)
-  CODAG_HD void put_aligned(const uint64_t* d, uint32_t n, uint8_t bits) {
+  template <class D>
+  CODAG_HD void put_aligned(const D& d, uint32_t n, uint8_t bits) {
     if (bits < 8) {
       const uint8_t mask = static_cast<uint8_t>((1 << bits) - 1);
       const uint32_t per_byte = 8 / bits;
@@ -359,14 +359,14 @@ class RleV2Writer {
       for (uint32_t i = 0; i < full; i += per_byte) {
         uint8_t b = 0;
         for (uint32_t j = 0; j < per_byte; ++j)
-          b |= static_cast<uint8_t>((d[i + j] & mask) << (8 - (j + 1) * bits));
+          b |= static_cast<uint8_t>((d(i + j) & mask) << (8 - (j + 1) * bits));
         put(b);
       }
       if (rem > 0) {
         uint32_t shift = 8 - bits;
         uint8_t b = 0;
         for (uint32_t i = full; i < n; ++i) {
-          b |= static_cast<uint8_t>((d[i] & mask) << shift);
+          b |= static_cast<uint8_t>((d(i) & mask) << shift);
           shift -= bits;
         }
         put(b);
@@ -374,16 +374,17 @@ class RleV2Writer {
     } else {
       const int bytes = bits / 8;
       for (uint32_t i = 0; i < n; ++i)
-        for (int j = bytes - 1; j >= 0; --j) put(static_cast<uint8_t>((d[i] >> (j * 8)) & 0xff));
+        for (int j = bytes - 1; j >= 0; --j) put(static_cast<uint8_t>((d(i) >> (j * 8)) & 0xff));
     }
   }
 
   // MSB-first packing at any width (write_unaligned_ints)
-  CODAG_HD void put_unaligned(const uint64_t* d, uint32_t n, uint8_t bits) {
+  template <class D>
+  CODAG_HD void put_unaligned(const D& d, uint32_t n, uint8_t bits) {
     uint32_t room = 8;
     uint8_t cur = 0;
     for (uint32_t i = 0; i < n; ++i) {
-      uint64_t value = d[i];
+      uint64_t value = d(i);
       uint32_t todo = bits;
       while (todo > room) {
         cur |= static_cast<uint8_t>(value >> (todo - room));
@@ -428,7 +429,8 @@ class RleV2Writer {
 
   CODAG_HD void write_direct() {
     uint8_t hist[32];
-    width_hist(lit_, nlit_, hist);
+    const auto lit = [this](uint32_t i) { return lit_[i]; };
+    width_hist(lit, nlit_, hist);
     const uint8_t bits = v2_closest_aligned(percentile_width(hist, nlit_, 100));
     const uint16_t enc = v2_code(bits);
     // The reference writes var_runlen-1 here.  On every path var_runlen equals the number
@@ -439,7 +441,7 @@ class RleV2Writer {
     const uint16_t len = static_cast<uint16_t>(nlit_ - 1);
     put(static_cast<uint8_t>(0x40 | (enc << 1) | ((len & 0x100) >> 8)));
     put(static_cast<uint8_t>(len & 0xff));
-    put_aligned(lit_, nlit_, bits);
+    put_aligned(lit, nlit_, bits);
     var_ = 0;
     nlit_ = 0;
   }
@@ -465,15 +467,16 @@ class RleV2Writer {
     put(static_cast<uint8_t>(0xC0 | (enc << 1) | ((len & 0x100) >> 8)));
     put(static_cast<uint8_t>(len & 0xff));
     put_uvarint(static_cast<int64_t>(lit_[0]));
-    put_svarint(static_cast<int64_t>(deltas_[0]));
-    if (!fixed_delta_) put_aligned(deltas_ + 1, nlit_ - 2, bits);
-    for (uint32_t i = 0; i < nlit_; ++i) deltas_[i] = 0;
+    // every path here has at least three pending values; a fixed run's deltas are all zero
+    put_svarint(static_cast<int64_t>(lit_[1] - lit_[0]));
+    if (!fixed_delta_) put_aligned([this](uint32_t i) { return lit_[i + 2] - lit_[i + 1]; }, nlit_ - 2, bits);
     nlit_ = 0;
     var_ = 0;
   }
 
-  CODAG_HD void write_patched(uint64_t lit_min, uint8_t b95, uint8_t b100, uint64_t* reduced) {
-    // patch list (preparePatchedBlob1, encoder.h:182-268)
+  CODAG_HD void write_patched(uint64_t lit_min, uint8_t b95, uint8_t b100) {
+    // patch list (preparePatchedBlob1, encoder.h:182-268); a group holds at most 128 values, so
+    // every gap is below 256 and each patch takes one list entry
     int64_t mask = static_cast<int64_t>((static_cast<uint64_t>(1) << b95) - 1);
     uint32_t pwidth = v2_closest(b100 - b95);
     if (pwidth == 64) {
@@ -481,41 +484,20 @@ class RleV2Writer {
       b95 = 8;
       mask = static_cast<int64_t>((static_cast<uint64_t>(1) << b95) - 1);
     }
-    uint64_t gaps[kMaxLiterals], patches[kMaxLiterals], list[kMaxLiterals];
+    uint64_t list[kMaxLiterals];
     uint32_t npatch = 0;
     size_t prev = 0, max_gap = 0;
     for (size_t i = 0; i < nlit_; i++) {
-      if (reduced[i] > static_cast<uint64_t>(mask)) {
-        size_t gap = i - prev;
+      const uint64_t r = lit_[i] - lit_min;
+      if (r > static_cast<uint64_t>(mask)) {
+        const size_t gap = i - prev;
         if (gap > max_gap) max_gap = gap;
         prev = i;
-        gaps[npatch] = gap;
-        patches[npatch] = reduced[i] >> b95;
-        npatch++;
-        reduced[i] &= static_cast<uint64_t>(mask);
+        list[npatch++] = (static_cast<uint64_t>(gap) << pwidth) | (r >> b95);
       }
     }
-    uint32_t gap_width;
-    if (max_gap == 0 && npatch != 0)
-      gap_width = 1;
-    else
-      gap_width = closest_width(max_gap);
-    uint32_t nlist = npatch;
-    if (gap_width > 8) {  // unreachable with 128-value groups; kept for format fidelity
-      gap_width = 8;
-      nlist += (max_gap == 511) ? 2 : 1;
-    }
-    uint32_t pos = 0;
-    for (uint32_t i = 0, gi = 0; i < nlist; i++) {
-      uint64_t g = gaps[gi], p = patches[gi];
-      gi++;
-      while (g > 255) {
-        list[pos++] = 255ull << pwidth;
-        i++;
-        g -= 255;
-      }
-      list[pos++] = (g << pwidth) | p;
-    }
+    const uint32_t gap_width = (max_gap == 0 && npatch != 0) ? 1u : closest_width(max_gap);
+    const uint32_t nlist = npatch;
 
     // header and body (writePatchedBasedValues, encoder.h:527-591)
     uint32_t len = var_ - 1;
@@ -530,8 +512,10 @@ class RleV2Writer {
     put(h2);
     put(h3);
     for (int i = static_cast<int>(base_bytes) - 1; i >= 0; i--) put(static_cast<uint8_t>((lit_min >> (i * 8)) & 0xff));
-    put_unaligned(reduced, nlit_, v2_closest(b95));
-    put_unaligned(list, nlist, v2_closest(gap_width + pwidth));
+    // base-reduced values; the patched ones keep their low b95 bits
+    put_unaligned([this, lit_min, mask](uint32_t i) { return (lit_[i] - lit_min) & static_cast<uint64_t>(mask); },
+                  nlit_, v2_closest(b95));
+    put_unaligned([&list](uint32_t i) { return list[i]; }, nlist, v2_closest(gap_width + pwidth));
     var_ = 0;
     nlit_ = 0;
   }
@@ -555,10 +539,8 @@ class RleV2Writer {
       increasing &= (l0 <= l1);
       decreasing &= (l0 >= l1);
       fixed_delta_ &= (d == initial);
-      deltas_[i - 1] = d;
       max_delta = d > max_delta ? d : max_delta;
     }
-    deltas_[0] = lit_[1] - lit_[0];
     // is_safe_subtract on unsigned values: only a minimum of 0 with maximum <= 128 fails
     const bool safe = (lmin > 0) || (lmax > static_cast<uint64_t>(lmin - INT8_MIN));
     if (!safe) {
@@ -577,17 +559,15 @@ class RleV2Writer {
       }
     }
     uint8_t hist[32];
-    width_hist(lit_, nlit_, hist);
+    width_hist([this](uint32_t i) { return lit_[i]; }, nlit_, hist);
     const uint8_t b100 = percentile_width(hist, nlit_, 100);
     const uint8_t b90 = percentile_width(hist, nlit_, 90);
     if (static_cast<uint32_t>(b100 - b90) > 1) {
-      uint64_t reduced[kMaxLiterals];
-      for (uint32_t i = 0; i < nlit_; i++) reduced[i] = lit_[i] - lmin;
-      width_hist(reduced, nlit_, hist);
+      width_hist([this, lmin](uint32_t i) { return lit_[i] - lmin; }, nlit_, hist);
       const uint8_t r95 = percentile_width(hist, nlit_, 95);
       const uint8_t r100 = percentile_width(hist, nlit_, 100);
       if (r100 - r95 != 0) {
-        write_patched(lmin, r95, r100, reduced);
+        write_patched(lmin, r95, r100);
       } else {
         write_direct();
       }
@@ -598,7 +578,6 @@ class RleV2Writer {
 
   Sink& out_;
   uint64_t lit_[kMaxLiterals] = {};
-  uint64_t deltas_[kMaxLiterals];
   uint32_t nlit_ = 0, fix_ = 0, var_ = 0;
   uint8_t delta_bits_ = 0;
   bool fixed_delta_ = false;
