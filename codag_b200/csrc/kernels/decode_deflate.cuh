@@ -282,7 +282,10 @@ struct TokenPipe {
     n = 0;
   }
   __device__ __forceinline__ void push(uint32_t t) {
-    if (lane == 0) sh->tok[k][n] = t;
+    // lane 0 writes the token: a predicated store, no branch on the lane
+    const uint32_t a = smem_u32(&sh->tok[k][n]);
+    asm volatile("{ .reg .pred p; setp.eq.u32 p, %0, 0; @p st.shared.u32 [%1], %2; }" ::"r"(lane), "r"(a), "r"(t)
+                 : "memory");
     if (++n == kTokBatch) handoff();
   }
   // one literal, or two (second in bits 8-15 when `two`)
@@ -607,6 +610,7 @@ template <class OUT>
 __device__ int expand_tokens(TokenShared* sh, uint32_t bar, OUT& out, uint32_t lane) {
   static_assert(OUT::kBytes - OUT::kFlush >= 258, "window too small for a match");
   uint32_t op = 0, k = 0;
+  const uint32_t tok_sh = 8u * (lane & 1u);  // a literal token: first byte in bits 0-7, second in 8-15
   uint32_t pend_op = 0, pend_len = 0, pend_end = 0, pend_val = 0;
 #define CODAG_COMPLETE()                                     \
   if (pend_len) {                                            \
@@ -620,9 +624,12 @@ __device__ int expand_tokens(TokenShared* sh, uint32_t bar, OUT& out, uint32_t l
     const uint32_t s_tok = smem_u32(sh->tok[k]);
     for (uint32_t i = 0; i < cnt; i++) {
       const uint32_t t = ld_s32(s_tok + 4u * i);
-      if (t >> 31) {  // literals
+      if (t >> 31) {  // literals: lane 0 stores the first, lane 1 the second (predicated)
         const uint32_t two = (t >> 16) & 1u;
-        if (lane <= two) out.put8(op + lane, lane ? (t >> 8) & 0xffu : t & 0xffu);
+        const uint32_t a = out.sbuf + ((op + lane) & OUT::kMask);
+        asm volatile("{ .reg .pred p; setp.le.u32 p, %0, %1; @p st.shared.u8 [%2], %3; }" ::"r"(lane), "r"(two),
+                     "r"(a), "r"(t >> tok_sh)
+                     : "memory");
         op += 1u + two;
       } else {
         const uint32_t len = t & 0x1ffu, dist = (t >> 9) & 0xffffu;

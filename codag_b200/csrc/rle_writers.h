@@ -237,10 +237,132 @@ CODAG_HD uint8_t closest_width(uint64_t v) {
   return static_cast<uint8_t>(v2_closest(c));
 }
 
-template <class Sink>
+// The RLE v2 writer's work on a closed group of up to 128 pending values, run by one thread: the
+// host producers.  A warp can stand in for it (the GPU encoder, one warp per chunk): it keeps
+// the pending values and the patch list where all its lanes see them and splits each operation
+// over its lanes, while every lane runs the writer's decisions on the same data.
+struct SerialGroups {
+  uint64_t lit[kMaxLiterals] = {};
+  uint64_t list[kMaxLiterals];
+  CODAG_HD uint64_t* lits() { return lit; }
+  CODAG_HD uint64_t* lists() { return list; }
+
+  struct Scan {
+    uint64_t lmin, lmax, max_delta;
+    bool increasing, decreasing, fixed;
+  };
+  // over l[0..n), n >= 2: extremes, monotonicity, whether every step equals the first, the largest
+  // step (steps as unsigned differences)
+  CODAG_HD Scan scan(const uint64_t* l, uint32_t n) const {
+    Scan r{l[0], l[0], 0, true, true, true};
+    const uint64_t initial = l[1] - l[0];
+    for (uint32_t i = 1; i < n; i++) {
+      const uint64_t l1 = l[i], l0 = l[i - 1];
+      const uint64_t d = l1 - l0;
+      r.lmin = l1 < r.lmin ? l1 : r.lmin;
+      r.lmax = l1 > r.lmax ? l1 : r.lmax;
+      r.increasing &= (l0 <= l1);
+      r.decreasing &= (l0 >= l1);
+      r.fixed &= (d == initial);
+      r.max_delta = d > r.max_delta ? d : r.max_delta;
+    }
+    return r;
+  }
+
+  // histogram of representable widths (compute_bit_width)
+  template <class D>
+  CODAG_HD void hist(const D& d, uint32_t n, uint8_t* h) const {
+    for (int i = 0; i < 32; i++) h[i] = 0;
+    for (uint32_t i = 0; i < n; ++i) h[v2_code(closest_width(d(i)))]++;
+  }
+
+  // fixed width big-endian packing used by DIRECT and DELTA (write_aligned_ints)
+  template <class S, class D>
+  CODAG_HD void pack_aligned(S& out, const D& d, uint32_t n, uint8_t bits) const {
+    if (bits < 8) {
+      const uint8_t mask = static_cast<uint8_t>((1 << bits) - 1);
+      const uint32_t per_byte = 8 / bits;
+      const uint32_t rem = n % per_byte;
+      const uint32_t full = n - rem;
+      for (uint32_t i = 0; i < full; i += per_byte) {
+        uint8_t b = 0;
+        for (uint32_t j = 0; j < per_byte; ++j)
+          b |= static_cast<uint8_t>((d(i + j) & mask) << (8 - (j + 1) * bits));
+        out.put(b);
+      }
+      if (rem > 0) {
+        uint32_t shift = 8 - bits;
+        uint8_t b = 0;
+        for (uint32_t i = full; i < n; ++i) {
+          b |= static_cast<uint8_t>((d(i) & mask) << shift);
+          shift -= bits;
+        }
+        out.put(b);
+      }
+    } else {
+      const int bytes = bits / 8;
+      for (uint32_t i = 0; i < n; ++i)
+        for (int j = bytes - 1; j >= 0; --j) out.put(static_cast<uint8_t>((d(i) >> (j * 8)) & 0xff));
+    }
+  }
+
+  // MSB-first packing at any width (write_unaligned_ints)
+  template <class S, class D>
+  CODAG_HD void pack_unaligned(S& out, const D& d, uint32_t n, uint8_t bits) const {
+    uint32_t room = 8;
+    uint8_t cur = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+      uint64_t value = d(i);
+      uint32_t todo = bits;
+      while (todo > room) {
+        cur |= static_cast<uint8_t>(value >> (todo - room));
+        todo -= room;
+        value &= (static_cast<uint64_t>(1) << todo) - 1;
+        out.put(cur);
+        cur = 0;
+        room = 8;
+      }
+      room -= todo;
+      cur |= static_cast<uint8_t>(value << room);
+      if (room == 0) {
+        out.put(cur);
+        cur = 0;
+        room = 8;
+      }
+    }
+    if (room != 8) out.put(cur);
+  }
+
+  // patch list of a PATCHED_BASE group (preparePatchedBlob1, encoder.h:182-268): one entry
+  // (gap << pwidth) | (value >> b95) per base-reduced value above mask, gaps from the previous
+  // patched position (0 before the first); a group holds at most 128 values, so every gap is
+  // below 256 and takes one entry.  Returns the entry count and the largest gap.
+  CODAG_HD uint32_t patches(const uint64_t* l, uint32_t n, uint64_t lmin, uint64_t mask, uint32_t b95,
+                            uint32_t pwidth, uint64_t* out, uint64_t* max_gap) const {
+    uint32_t np = 0;
+    uint64_t prev = 0, mg = 0;
+    for (uint32_t i = 0; i < n; i++) {
+      const uint64_t r = l[i] - lmin;
+      if (r > mask) {
+        const uint64_t gap = i - prev;
+        if (gap > mg) mg = gap;
+        prev = i;
+        out[np++] = (gap << pwidth) | (r >> b95);
+      }
+    }
+    *max_gap = mg;
+    return np;
+  }
+};
+
+template <class Sink, class G = SerialGroups>
 class RleV2Writer {
  public:
-  CODAG_HD explicit RleV2Writer(Sink& out) : out_(out) {}
+  CODAG_HD explicit RleV2Writer(Sink& out) : out_(out), lit_(g_.lits()) {}
+  // a group executor with its own storage (one warp per chunk)
+  CODAG_HD RleV2Writer(Sink& out, const G& g) : out_(out), g_(g), lit_(g_.lits()) {}
+  RleV2Writer(const RleV2Writer&) = delete;  // lit_ points into g_
+  RleV2Writer& operator=(const RleV2Writer&) = delete;
 
   // n values, value i read as get(i) (zero-extended to 64 bits)
   template <class Get>
@@ -327,15 +449,7 @@ class RleV2Writer {
   CODAG_HD void put(uint8_t b) { out_.put(b); }
 
   // The writer keeps only the pending values (lit_) and the patch list: deltas and base-reduced
-  // values are derived from lit_ where they are read, which keeps a GPU thread's state small
-  // enough for L1.  d(i) below is any such derived sequence.
-
-  // histogram of representable widths (compute_bit_width)
-  template <class D>
-  CODAG_HD static void width_hist(const D& d, uint32_t n, uint8_t* hist) {
-    for (int i = 0; i < 32; i++) hist[i] = 0;
-    for (uint32_t i = 0; i < n; ++i) hist[v2_code(closest_width(d(i)))]++;
-  }
+  // values are derived from lit_ where they are read, which keeps a GPU thread's state small.
 
   // smallest width covering all but the top (100-p)% of values (compute_percentile_bit_width)
   CODAG_HD static uint8_t percentile_width(const uint8_t* hist, uint32_t n, uint8_t p) {
@@ -346,63 +460,6 @@ class RleV2Writer {
       if (left < 0) return v2_width(i);
     }
     return 0;
-  }
-
-  // fixed width big-endian packing used by DIRECT and DELTA (write_aligned_ints)
-  template <class D>
-  CODAG_HD void put_aligned(const D& d, uint32_t n, uint8_t bits) {
-    if (bits < 8) {
-      const uint8_t mask = static_cast<uint8_t>((1 << bits) - 1);
-      const uint32_t per_byte = 8 / bits;
-      const uint32_t rem = n % per_byte;
-      const uint32_t full = n - rem;
-      for (uint32_t i = 0; i < full; i += per_byte) {
-        uint8_t b = 0;
-        for (uint32_t j = 0; j < per_byte; ++j)
-          b |= static_cast<uint8_t>((d(i + j) & mask) << (8 - (j + 1) * bits));
-        put(b);
-      }
-      if (rem > 0) {
-        uint32_t shift = 8 - bits;
-        uint8_t b = 0;
-        for (uint32_t i = full; i < n; ++i) {
-          b |= static_cast<uint8_t>((d(i) & mask) << shift);
-          shift -= bits;
-        }
-        put(b);
-      }
-    } else {
-      const int bytes = bits / 8;
-      for (uint32_t i = 0; i < n; ++i)
-        for (int j = bytes - 1; j >= 0; --j) put(static_cast<uint8_t>((d(i) >> (j * 8)) & 0xff));
-    }
-  }
-
-  // MSB-first packing at any width (write_unaligned_ints)
-  template <class D>
-  CODAG_HD void put_unaligned(const D& d, uint32_t n, uint8_t bits) {
-    uint32_t room = 8;
-    uint8_t cur = 0;
-    for (uint32_t i = 0; i < n; ++i) {
-      uint64_t value = d(i);
-      uint32_t todo = bits;
-      while (todo > room) {
-        cur |= static_cast<uint8_t>(value >> (todo - room));
-        todo -= room;
-        value &= (static_cast<uint64_t>(1) << todo) - 1;
-        put(cur);
-        cur = 0;
-        room = 8;
-      }
-      room -= todo;
-      cur |= static_cast<uint8_t>(value << room);
-      if (room == 0) {
-        put(cur);
-        cur = 0;
-        room = 8;
-      }
-    }
-    if (room != 8) put(cur);
   }
 
   CODAG_HD void put_uvarint(int64_t val) {
@@ -429,8 +486,9 @@ class RleV2Writer {
 
   CODAG_HD void write_direct() {
     uint8_t hist[32];
-    const auto lit = [this](uint32_t i) { return lit_[i]; };
-    width_hist(lit, nlit_, hist);
+    const uint64_t* l = lit_;
+    const auto lit = [l](uint32_t i) { return l[i]; };
+    g_.hist(lit, nlit_, hist);
     const uint8_t bits = v2_closest_aligned(percentile_width(hist, nlit_, 100));
     const uint16_t enc = v2_code(bits);
     // The reference writes var_runlen-1 here.  On every path var_runlen equals the number
@@ -441,7 +499,7 @@ class RleV2Writer {
     const uint16_t len = static_cast<uint16_t>(nlit_ - 1);
     put(static_cast<uint8_t>(0x40 | (enc << 1) | ((len & 0x100) >> 8)));
     put(static_cast<uint8_t>(len & 0xff));
-    put_aligned(lit, nlit_, bits);
+    g_.pack_aligned(out_, lit, nlit_, bits);
     var_ = 0;
     nlit_ = 0;
   }
@@ -469,7 +527,10 @@ class RleV2Writer {
     put_uvarint(static_cast<int64_t>(lit_[0]));
     // every path here has at least three pending values; a fixed run's deltas are all zero
     put_svarint(static_cast<int64_t>(lit_[1] - lit_[0]));
-    if (!fixed_delta_) put_aligned([this](uint32_t i) { return lit_[i + 2] - lit_[i + 1]; }, nlit_ - 2, bits);
+    if (!fixed_delta_) {
+      const uint64_t* l = lit_;
+      g_.pack_aligned(out_, [l](uint32_t i) { return l[i + 2] - l[i + 1]; }, nlit_ - 2, bits);
+    }
     nlit_ = 0;
     var_ = 0;
   }
@@ -484,18 +545,9 @@ class RleV2Writer {
       b95 = 8;
       mask = static_cast<int64_t>((static_cast<uint64_t>(1) << b95) - 1);
     }
-    uint64_t list[kMaxLiterals];
-    uint32_t npatch = 0;
-    size_t prev = 0, max_gap = 0;
-    for (size_t i = 0; i < nlit_; i++) {
-      const uint64_t r = lit_[i] - lit_min;
-      if (r > static_cast<uint64_t>(mask)) {
-        const size_t gap = i - prev;
-        if (gap > max_gap) max_gap = gap;
-        prev = i;
-        list[npatch++] = (static_cast<uint64_t>(gap) << pwidth) | (r >> b95);
-      }
-    }
+    uint64_t* list = g_.lists();
+    uint64_t max_gap = 0;
+    const uint32_t npatch = g_.patches(lit_, nlit_, lit_min, static_cast<uint64_t>(mask), b95, pwidth, list, &max_gap);
     const uint32_t gap_width = (max_gap == 0 && npatch != 0) ? 1u : closest_width(max_gap);
     const uint32_t nlist = npatch;
 
@@ -513,9 +565,10 @@ class RleV2Writer {
     put(h3);
     for (int i = static_cast<int>(base_bytes) - 1; i >= 0; i--) put(static_cast<uint8_t>((lit_min >> (i * 8)) & 0xff));
     // base-reduced values; the patched ones keep their low b95 bits
-    put_unaligned([this, lit_min, mask](uint32_t i) { return (lit_[i] - lit_min) & static_cast<uint64_t>(mask); },
-                  nlit_, v2_closest(b95));
-    put_unaligned([&list](uint32_t i) { return list[i]; }, nlist, v2_closest(gap_width + pwidth));
+    const uint64_t* l = lit_;
+    const uint64_t um = static_cast<uint64_t>(mask);
+    g_.pack_unaligned(out_, [l, lit_min, um](uint32_t i) { return (l[i] - lit_min) & um; }, nlit_, v2_closest(b95));
+    g_.pack_unaligned(out_, [list](uint32_t i) { return list[i]; }, nlist, v2_closest(gap_width + pwidth));
     var_ = 0;
     nlit_ = 0;
   }
@@ -526,21 +579,11 @@ class RleV2Writer {
       write_direct();
       return;
     }
-    bool increasing = true, decreasing = true;
-    fixed_delta_ = true;
-    uint64_t lmin = lit_[0], lmax = lit_[0];
+    const typename G::Scan sc = g_.scan(lit_, nlit_);
+    const uint64_t lmin = sc.lmin, lmax = sc.lmax, max_delta = sc.max_delta;
     const uint64_t initial = lit_[1] - lit_[0];
-    uint64_t max_delta = 0;
-    for (uint32_t i = 1; i < nlit_; i++) {
-      const uint64_t l1 = lit_[i], l0 = lit_[i - 1];
-      const uint64_t d = l1 - l0;
-      lmin = l1 < lmin ? l1 : lmin;
-      lmax = l1 > lmax ? l1 : lmax;
-      increasing &= (l0 <= l1);
-      decreasing &= (l0 >= l1);
-      fixed_delta_ &= (d == initial);
-      max_delta = d > max_delta ? d : max_delta;
-    }
+    const bool increasing = sc.increasing, decreasing = sc.decreasing;
+    fixed_delta_ = sc.fixed;
     // is_safe_subtract on unsigned values: only a minimum of 0 with maximum <= 128 fails
     const bool safe = (lmin > 0) || (lmax > static_cast<uint64_t>(lmin - INT8_MIN));
     if (!safe) {
@@ -559,11 +602,12 @@ class RleV2Writer {
       }
     }
     uint8_t hist[32];
-    width_hist([this](uint32_t i) { return lit_[i]; }, nlit_, hist);
+    const uint64_t* l = lit_;
+    g_.hist([l](uint32_t i) { return l[i]; }, nlit_, hist);
     const uint8_t b100 = percentile_width(hist, nlit_, 100);
     const uint8_t b90 = percentile_width(hist, nlit_, 90);
     if (static_cast<uint32_t>(b100 - b90) > 1) {
-      width_hist([this, lmin](uint32_t i) { return lit_[i] - lmin; }, nlit_, hist);
+      g_.hist([l, lmin](uint32_t i) { return l[i] - lmin; }, nlit_, hist);
       const uint8_t r95 = percentile_width(hist, nlit_, 95);
       const uint8_t r100 = percentile_width(hist, nlit_, 100);
       if (r100 - r95 != 0) {
@@ -577,7 +621,8 @@ class RleV2Writer {
   }
 
   Sink& out_;
-  uint64_t lit_[kMaxLiterals] = {};
+  G g_;
+  uint64_t* lit_;
   uint32_t nlit_ = 0, fix_ = 0, var_ = 0;
   uint8_t delta_bits_ = 0;
   bool fixed_delta_ = false;

@@ -3,6 +3,8 @@ host producers' (codag_encode_rlev1/_rlev2, whose RLE v2 bytes are pinned to COD
 encoder by tests/test_golden_rlev2.py), for every element width, for inputs whose size is not
 a multiple of the element or the chunk, and for CODAG-written columns; and they decode back
 through the CUDA decoders."""
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -33,6 +35,24 @@ def test_gpu_encoder_matches_host_producer(cuda, native, codec, e):
         assert np.array_equal(off.cpu().numpy().view(np.uint64), w_off)
         assert np.array_equal(ln.cpu().numpy().view(np.uint64), w_len)
         assert np.array_equal(f.cpu().numpy(), want), (codec, e, raw.size)
+
+
+GOLDEN = sorted(p.stem for p in (Path(__file__).parent / "golden").glob("ref_rlev2_*.npz") if p.stem != "ref_rlev2_tables")
+
+
+@pytest.mark.parametrize("name", GOLDEN)
+def test_gpu_rlev2_encoder_on_codag_columns(cuda, native, name):
+    """The columns of CODAG's golden RLE v2 files (every header kind, patches wider than 32 bits,
+    runs of zeros, every element width): one warp per chunk writes the host producer's bytes."""
+    from codag_b200 import api
+    g = np.load(Path(__file__).parent / "golden" / f"{name}.npz")
+    e = int(g["elem"])
+    raw = np.ascontiguousarray(g["src"]).view(np.uint8)
+    want, w_off, w_len = native.encode_rlev2(raw, CH, e)
+    f, off, ln = api.compress_rle(native.RLEV2, cuda.from_numpy(raw.copy()).to("cuda"), CH, e)
+    assert np.array_equal(ln.cpu().numpy().view(np.uint64), w_len)
+    assert np.array_equal(off.cpu().numpy().view(np.uint64), w_off)
+    assert np.array_equal(f.cpu().numpy(), want), name
 
 
 @pytest.mark.parametrize("codec", [0, 1], ids=["rlev1", "rlev2"])
