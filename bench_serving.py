@@ -60,6 +60,15 @@ def main(args, rank: int, world: int, local: int) -> None:
         reqs = srv.run(arr, time_limit=args.duration * 3 + 30)
         s = serving.summarize(reqs, pool, args.duration)
         s["rate"] = rate
+        if world > 1:  # one replica per GPU: the job's throughput is the sum, its latency the worst
+            import torch.distributed as dist
+            t = torch.tensor([s["gbs"], s["p50_ms"], s["p99_ms"], 0.0 if s["bit_exact"] else 1.0],
+                             dtype=torch.float64, device=f"cuda:{local}")
+            tot = t.clone()
+            dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            s.update(gbs=float(tot[0]), p50_ms=float(t[1]), p99_ms=float(t[2]), bit_exact=float(t[3]) == 0.0,
+                     replicas=world)
         rows.append(s)
         if rank == 0:
             print(json.dumps({"serving_rate": rate, **s}), flush=True)
