@@ -13,6 +13,19 @@ import json
 SEED = 20260105
 
 
+def _shape(args, srv):
+    """The serving loop's launch shape: --tune if given, else the serving tuner (cached per GPU
+    model unless --autotune search), else the library default (--autotune '')."""
+    from codag_b200 import native, serving
+    if args.tune:
+        shape = tuple(int(x) for x in args.tune.split(","))[:4]
+        srv.tune = native.Tune(*shape, 0)
+        return shape
+    if args.autotune:
+        return serving.tune_server(srv, use_cache=args.autotune == "cached")
+    return None
+
+
 def short_sweep(args, local: int, rates=(500.0, 2000.0), duration: float = 10.0, pool_files: int = 24) -> dict:
     """A short sweep for the default bench line: `rates` for `duration` seconds each over a
     pool of `pool_files` files; returns decompressed GB/s and p50/p99 latency per rate."""
@@ -23,6 +36,7 @@ def short_sweep(args, local: int, rates=(500.0, 2000.0), duration: float = 10.0,
     pool = serving.build_pool(pool_files, SEED)
     srv = serving.Server(pool, args.budget_gb << 30, slots=args.slots, device=f"cuda:{local}")
     srv.run(serving.poisson_arrivals(50, 0.5, len(pool.files), 1))
+    shape = _shape(args, srv)
     rows = []
     for k, rate in enumerate(rates):
         arr = serving.poisson_arrivals(rate, duration, len(pool.files), SEED + 17 * k)
@@ -34,7 +48,7 @@ def short_sweep(args, local: int, rates=(500.0, 2000.0), duration: float = 10.0,
                        f"log-uniform 64 KiB-256 MiB (mean {sum(sizes) / len(sizes) / 1e6:.1f} MB), "
                        "40/30/30 Deflate/RLE v1/RLE v2, 128 KiB chunks",
            "budget_bytes": args.budget_gb << 30, "rates": rows, "bit_exact": all(r["bit_exact"] for r in rows),
-           "launches": srv.launches}
+           "launches": srv.launches, "tune": list(shape) if shape else None}
     del srv, pool
     torch.cuda.empty_cache()
     return out
@@ -50,6 +64,7 @@ def main(args, rank: int, world: int, local: int) -> None:
     srv = serving.Server(pool, args.budget_gb << 30, slots=args.slots, device=f"cuda:{local}")
     warm = serving.poisson_arrivals(50, 0.5, len(pool.files), 1)
     srv.run(warm)
+    shape = _shape(args, srv)
     rates = [float(x) for x in args.rates.split(",")]
     rows = []
     clocks = Clocks(local) if rank == 0 else None
@@ -85,7 +100,8 @@ def main(args, rank: int, world: int, local: int) -> None:
         "config": {"workload": f"serving: Poisson arrivals, {args.duration:g} s per rate, pool of {len(pool.files)} files "
                                f"log-uniform 64 KiB-256 MiB (mean {sum(sizes) / len(sizes) / 1e6:.1f} MB), "
                                "40/30/30 Deflate/RLE v1/RLE v2, 128 KiB chunks",
-                   "budget_bytes": args.budget_gb << 30, "slots": args.slots},
+                   "budget_bytes": args.budget_gb << 30, "slots": args.slots,
+                   "tune": list(shape) if shape else None},
         "bit_exact": all(r["bit_exact"] for r in rows),
         "rates": rows, "launches": srv.launches, "gpu_launches": srv.launches,
         "clocks": clk,

@@ -167,6 +167,39 @@ def poisson_arrivals(rate: float, duration: float, n_files: int, seed: int):
     return list(zip(t.tolist(), rng.integers(0, n_files, t.size).tolist()))
 
 
+# Launch shapes (warps_per_cta, ring_slots, lut_bits, cta_per_chunk) tried by tune_server.  The
+# per-file Deflate default (2 warps per CTA) holds too few warps per SM for a loop whose launches
+# carry thousands of 128 KiB chunks: 36.6 GB/s against 60.0 GB/s with 8 warps per CTA at
+# 2000 requests per second on one B200.
+SERVE_SHAPES = [(w, 4, lb, 0) for w in (2, 4, 8) for lb in (9, 10)]
+
+
+def tune_server(srv: "Server", n_requests: int = 96, seed: int = 7, use_cache: bool = True):
+    """Times a burst of n_requests requests that all arrive at once (the loop saturated) for each
+    shape of SERVE_SHAPES, installs the fastest on `srv` and returns it; the result is cached per
+    GPU model next to the decoders' (codag_b200.tuning)."""
+    from . import tuning
+    hit = tuning.load_cached(-1, "serve") if use_cache else None
+    if hit:
+        srv.tune = native.Tune(*hit, 0)
+        return tuple(hit)
+    rng = np.random.default_rng(seed)
+    burst = [(0.0, int(f)) for f in rng.integers(0, len(srv.pool.files), n_requests)]
+    best, best_t = None, None
+    for shape in SERVE_SHAPES:
+        srv.tune = native.Tune(*shape, 0)
+        t0 = time.perf_counter()
+        reqs = srv.run(burst)
+        t = time.perf_counter() - t0
+        if not all(r.ok for r in reqs):
+            raise RuntimeError(f"serving shape {shape}: a request did not decode exactly")
+        if best_t is None or t < best_t:
+            best, best_t = shape, t
+    srv.tune = native.Tune(*best, 0)
+    tuning.store_cached(-1, "serve", best)
+    return best
+
+
 def admission_capacity(budget_bytes: int, free_bytes: int, reserve_bytes: int) -> int:
     """Output bytes the server may hold for admitted requests: the configured budget, but no
     more than the device memory that is free once the request pool is resident, less a

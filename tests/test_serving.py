@@ -110,3 +110,25 @@ def test_server_admits_by_free_device_memory(cuda, small_pool):
     assert srv.arena.capacity <= free - serving.Server.RESERVE
     reqs = srv.run(serving.poisson_arrivals(400, 0.05, len(pool.files), 3))
     assert reqs and all(r.ok for r in reqs)
+    del srv  # give the device memory back for the tests after this one
+    import gc
+    gc.collect()
+    cuda.cuda.empty_cache()
+
+
+@pytest.mark.gpu
+def test_tune_server_picks_a_listed_shape(cuda, small_pool, monkeypatch, tmp_path):
+    """The serving tuner times each listed launch shape on a saturating burst, keeps the fastest
+    (every request exact under every shape) and caches it."""
+    from codag_b200 import tuning
+    monkeypatch.setattr(tuning, "CACHE", tmp_path / "tune.json")
+    import gc
+    gc.collect()
+    cuda.cuda.empty_cache()
+    srv = serving.Server(small_pool, 1 << 30, slots=2, device="cuda")
+    shape = serving.tune_server(srv, n_requests=24, use_cache=False)
+    assert shape in serving.SERVE_SHAPES
+    assert tuple(tuning.load_cached(-1, "serve")) == shape
+    assert serving.tune_server(srv) == shape  # from the cache
+    reqs = srv.run([(0.0, f) for f in range(len(small_pool.files))])
+    assert all(r.ok for r in reqs)
