@@ -380,6 +380,7 @@ codag_status compress(const uint8_t* d_in, uint64_t in_bytes, uint64_t chunk, in
   if (!ws || ws_bytes < codag_compress_workspace_bytes(CODEC, in_bytes, chunk, e) ||
       (reinterpret_cast<uintptr_t>(ws) & 255u))
     return CODAG_EINVAL;
+  (void)cudaGetLastError();  // an error earlier work left pending is not this call's
   uint8_t* scratch = static_cast<uint8_t*>(ws);
   uint64_t* lens = reinterpret_cast<uint64_t*>(scratch + n * slot);
   if (d_status && cudaMemsetAsync(d_status, 0, sizeof(int32_t), s) != cudaSuccess) return CODAG_ECUDA;

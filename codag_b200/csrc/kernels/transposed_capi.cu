@@ -271,6 +271,7 @@ extern "C" codag_status codag_decompress_rlev2_transposed(const uint8_t* d_comp,
       (reinterpret_cast<uintptr_t>(d_out) % elem_bytes) || (reinterpret_cast<uintptr_t>(d_comp) & 3u))
     return CODAG_EINVAL;
   if (n_chunks == 0) return CODAG_OK;
+  (void)cudaGetLastError();  // an error earlier work left pending is not this call's
   const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   const uint32_t ru = static_cast<uint32_t>(read_unit);
   switch (elem_bytes) {

@@ -226,7 +226,7 @@ typedef struct {
 typedef struct codag_plan codag_plan;
 
 /* Copies the descriptors to the device (the only allocating call), orders the queue and
- * picks the launch shape (tune may be NULL: use the process-wide defaults).  In a plan,
+ * picks the launch shape (tune may be NULL: 8 warps per CTA, 4 ring slots, 10-bit tables).  In a plan,
  * tune->cta_per_chunk = k (1..4, warps_per_cta even) sends the Deflate chunks of at least
  * k x 256 KiB to warp pairs (a symbol decoder and a byte expander each), decoded first. */
 codag_status codag_batch_plan(const codag_chunk_desc *h_descs, uint64_t n, const codag_tune *tune,
@@ -243,7 +243,8 @@ codag_status codag_batch_destroy(codag_plan *plan);
  * that rebuild the chunk list for every launch (continuous batching).  d_order (n u32,
  * may be NULL = descriptor order) is the order the warps take chunks in; d_queue is 4 bytes
  * of device memory that this call resets on `stream`; d_status has n entries (may be NULL)
- * and entry i reports descriptor i.  tune may be NULL (process-wide defaults).  Allocates
+ * and entry i reports descriptor i.  tune may be NULL (8 warps per CTA, 4 ring slots, 10-bit
+ * tables, as codag_batch_plan).  Allocates
  * nothing; the launch shape of each tune is measured once per device and cached. */
 codag_status codag_batch_launch(const codag_chunk_desc *d_descs, const uint32_t *d_order, uint64_t n,
                                 uint32_t *d_queue, const codag_tune *tune, const uint8_t *d_comp,
