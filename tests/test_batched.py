@@ -221,3 +221,27 @@ def test_table_placement_is_a_plan_option(native):
     t = native.Tune(2, 2, 9, 0, 1)
     assert native.lib().codag_set_tune(native.DEFLATE, C.byref(t)) == native.EINVAL
     assert native.get_tune(native.DEFLATE).table_global == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_plans_sharing_a_kernel_at_different_warp_counts(cuda, small_set, use_graph):
+    """Plans of 8 and of 2 warps per CTA with the same ring depth and table width launch the same
+    kernel with different shared-memory sizes: making the small plan after the large one (and a
+    small unplanned launch in between) must leave the large plan launchable."""
+    from codag_b200 import api
+    ms = small_set
+    d_comp = cuda.from_numpy(ms.comp).to("cuda")
+    want = cuda.from_numpy(ms.expected()).to("cuda")
+    big = api.BatchPlan(ms.descs, 8, 4, 10)
+    small = api.BatchPlan(ms.descs, 2, 4, 10)
+    try:
+        for plan in (small, big, small, big):
+            out = cuda.zeros(ms.out_bytes, dtype=cuda.uint8, device="cuda")
+            st = cuda.full((ms.n,), -1, dtype=cuda.int32, device="cuda")
+            plan.run(d_comp, out, st, use_graph=use_graph)
+            cuda.cuda.synchronize()
+            assert int((st != 0).sum().item()) == 0 and bool(cuda.equal(out, want))
+    finally:
+        big.close()
+        small.close()
