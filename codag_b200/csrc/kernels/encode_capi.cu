@@ -128,7 +128,51 @@ struct WarpGroups {
   uint32_t* hs;    // 32 histogram counters (shared memory)
   uint32_t lane;
   using Scan = codag_fmt::SerialGroups::Scan;
+  static constexpr bool kBulk = true;
   __device__ uint64_t* lits() { return lit; }
+
+  // Up to min(32, lim) values i, i+1, ... that extend a variable run: lane k takes value i+k and
+  // its step from the value before; the run stops before the first value whose step and the
+  // step before it are both zero (the writer's fixed-run test) and at the end of the input.
+  // Appends the values taken to l[nl..], leaves the last step taken in prev_delta, and returns
+  // the count (0: the writer's per-value steps take value i).
+  template <class Get>
+  __device__ uint32_t append_run(const Get& get, uint64_t i, uint64_t n, uint64_t* l, uint32_t nl,
+                                 uint64_t& prev_delta, uint32_t lim) const {
+    __syncwarp();
+    const uint64_t j = i + lane;
+    const bool in = j < n;
+    const uint64_t v = in ? static_cast<uint64_t>(get(j)) : 0ull;
+    uint64_t before = __shfl_up_sync(FULL_MASK, v, 1);
+    if (lane == 0) before = l[nl - 1];
+    const uint64_t d = v - before;
+    const uint32_t zero = __ballot_sync(FULL_MASK, in && d == 0);
+    const uint32_t zero_before = (zero << 1) | (prev_delta == 0 ? 1u : 0u);
+    const uint32_t stop = (zero & zero_before) | __ballot_sync(FULL_MASK, !in);
+    uint32_t take = stop ? static_cast<uint32_t>(__ffs(stop)) - 1u : 32u;
+    if (take > lim) take = lim;
+    if (lane < take) l[nl + lane] = v;
+    if (take) prev_delta = __shfl_sync(FULL_MASK, d, static_cast<int>(take - 1));
+    __syncwarp();
+    return take;
+  }
+
+  // Up to min(32, lim) values i, i+1, ... equal to the last pending value (a fixed run going on),
+  // appended to l[nl..]; returns the count
+  template <class Get>
+  __device__ uint32_t append_equal(const Get& get, uint64_t i, uint64_t n, uint64_t* l, uint32_t nl,
+                                   uint32_t lim) const {
+    __syncwarp();
+    const uint64_t last = l[nl - 1];
+    const uint64_t j = i + lane;
+    const bool eq = j < n && static_cast<uint64_t>(get(j)) == last;
+    const uint32_t stop = __ballot_sync(FULL_MASK, !eq);
+    uint32_t take = stop ? static_cast<uint32_t>(__ffs(stop)) - 1u : 32u;
+    if (take > lim) take = lim;
+    if (lane < take) l[nl + lane] = last;
+    __syncwarp();
+    return take;
+  }
   __device__ uint64_t* lists() { return list; }
 
   __device__ Scan scan(const uint64_t* l, uint32_t n) const {

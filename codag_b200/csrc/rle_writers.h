@@ -242,6 +242,16 @@ CODAG_HD uint8_t closest_width(uint64_t v) {
 // the pending values and the patch list where all its lanes see them and splits each operation
 // over its lanes, while every lane runs the writer's decisions on the same data.
 struct SerialGroups {
+  // no bulk path: every value takes the writer's per-value steps (see RleV2Writer::encode)
+  static constexpr bool kBulk = false;
+  template <class Get>
+  CODAG_HD uint32_t append_run(const Get&, uint64_t, uint64_t, uint64_t*, uint32_t, uint64_t&, uint32_t) const {
+    return 0;
+  }
+  template <class Get>
+  CODAG_HD uint32_t append_equal(const Get&, uint64_t, uint64_t, uint64_t*, uint32_t, uint32_t) const {
+    return 0;
+  }
   uint64_t lit[kMaxLiterals] = {};
   uint64_t list[kMaxLiterals];
   CODAG_HD uint64_t* lits() { return lit; }
@@ -369,6 +379,37 @@ class RleV2Writer {
   CODAG_HD void encode(const Get& get, uint64_t n) {
     uint64_t prev_delta = 0;
     for (uint64_t i = 0; i < n; i++) {
+      if constexpr (G::kBulk) {
+        // Inside a variable run (no fixed run pending, two or more values held) a value only
+        // appends to the pending values, until two zero steps in a row start a fixed run or the
+        // group reaches 128 values: the executor may take such values many at a time.
+        if (fix_ == 0 && nlit_ >= 2) {
+          const uint32_t lim_v = static_cast<uint32_t>(kMaxLiterals) - var_;
+          const uint32_t lim_n = static_cast<uint32_t>(kMaxLiterals) - nlit_;
+          const uint32_t took = g_.append_run(get, i, n, lit_, nlit_, prev_delta, lim_v < lim_n ? lim_v : lim_n);
+          if (took) {
+            nlit_ += took;
+            var_ += took;
+            if (var_ == static_cast<uint32_t>(kMaxLiterals)) choose_encoding();
+            i += took - 1;  // the loop's increment moves to the first value not taken
+            continue;
+          }
+        }
+        // Inside a fixed run (no variable values pending) a value equal to the last only appends,
+        // until the run reaches 128 values.
+        if (var_ == 0 && fix_ >= static_cast<uint32_t>(kMinRepeat) && prev_delta == 0 && nlit_ >= 1) {
+          const uint32_t lim_f = static_cast<uint32_t>(kMaxLiterals) - fix_;
+          const uint32_t lim_n = static_cast<uint32_t>(kMaxLiterals) - nlit_;
+          const uint32_t took = g_.append_equal(get, i, n, lit_, nlit_, lim_f < lim_n ? lim_f : lim_n);
+          if (took) {
+            nlit_ += took;
+            fix_ += took;
+            if (fix_ == static_cast<uint32_t>(kMaxLiterals)) choose_encoding();
+            i += took - 1;
+            continue;
+          }
+        }
+      }
       const uint64_t val = get(i);
       if (nlit_ == 0) {
         lit_[nlit_++] = val;
