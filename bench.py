@@ -373,8 +373,7 @@ def measure_encode(workload: str, local: int, steps: int = 5) -> dict:
     torch.cuda.empty_cache()
     return {"workload": "GPU encode of " + w["desc"], "value": round(f["col"].size / dt / 1e9, 2), "unit": "GB/s",
             "ms_per_step": round(dt * 1e3, 3), "bit_exact_vs_host_producer": ok,
-            "how": ("codag_compress_rlev2: one warp per chunk" if codec == 1 else
-                    "codag_compress_rlev1: one thread per chunk") + ", scan, gather; input bytes per second"}
+            "how": f"codag_compress_rlev{codec + 1}: one warp per chunk, scan, gather; input bytes per second"}
 
 
 def _summary(line: dict) -> dict:

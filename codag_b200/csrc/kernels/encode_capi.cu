@@ -5,9 +5,9 @@
 // / deflate_orig, rlev2/encoder_trans.h:184-357 block_encode_orig driven by compress_gpu_orig
 // :482-564), then scans the stream lengths and moves every stream to its aligned offset.  The
 // same three steps run here as three kernels on the caller's stream:
-//   k_encode_chunks  RLE v1: one thread per chunk runs the shared writer of ../rle_writers.h (the
-//                    code the host producers run, so the bytes are the same) into its own slot
-//                    of the caller's workspace;
+//   k_encode_rlev1_warp  RLE v1: one warp per chunk runs the shared writer of ../rle_writers.h (the
+//                    code the host producers run, so the bytes are the same) into its own slot of
+//                    the caller's workspace, literal streams and runs 32 values at a time;
 //   k_encode_rlev2_warp  RLE v2: one warp per chunk runs the same writer, its group operations
 //                    split over the lanes (see below);
 //   k_scan_offsets   one CTA turns the stream lengths into the aligned offsets (blk_off);
@@ -26,20 +26,6 @@ namespace {
 
 constexpr uint64_t kOverflow = ~0ull;
 
-// writer output into a fixed slot; bytes past the slot are counted but not stored
-struct DevSink {
-  uint8_t* p;
-  uint64_t cap;
-  uint64_t n;
-  __device__ void put(uint8_t b) {
-    if (n < cap) p[n] = b;
-    n++;
-  }
-  __device__ uint64_t size() const { return n; }
-  __device__ void set(uint64_t i, uint8_t b) {
-    if (i < cap) p[i] = b;
-  }
-};
 
 // element j of one chunk of the input zero padded past in_bytes (d_in is element aligned)
 template <typename T>
@@ -69,25 +55,6 @@ struct Wide<uint32_t> { using T = unsigned int; };
 template <>
 struct Wide<uint64_t> { using T = unsigned long long; };
 
-template <int CODEC, typename T>
-__global__ void __launch_bounds__(32) k_encode_chunks(const uint8_t* __restrict__ in, uint64_t in_bytes,
-                                                      uint64_t chunk_bytes, uint64_t n, uint8_t* __restrict__ scratch,
-                                                      uint64_t slot, uint64_t* __restrict__ lens) {
-  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  DevSink s{scratch + i * slot, slot, 0};
-  using W = typename Wide<T>::T;
-  const PaddedChunk<W> g{in, in_bytes, i * chunk_bytes};
-  const uint64_t cnt = chunk_bytes / sizeof(T);
-  if constexpr (CODEC == CODAG_CODEC_RLEV1) {
-    codag_fmt::RleV1Writer<T, DevSink> w(s);
-    w.encode([&](uint64_t j) { return static_cast<T>(g(j)); }, cnt);
-  } else {
-    codag_fmt::RleV2Writer<DevSink> w(s);
-    w.encode([&](uint64_t j) { return static_cast<uint64_t>(g(j)); }, cnt);
-  }
-  lens[i] = s.n > slot ? kOverflow : s.n;
-}
 
 // ---------------------------------------------------------------------------------------
 // RLE v2, one warp per chunk.  With one thread per chunk the 32 threads of a warp take
@@ -114,6 +81,9 @@ struct WarpSink {
   }
   __device__ void advance(uint64_t k) { n += k; }
   __device__ uint64_t size() const { return n; }
+  __device__ void set(uint64_t i, uint8_t b) {
+    if (lane == 0 && i < cap) p[i] = b;
+  }
 };
 
 __device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return a < b ? a : b; }
@@ -292,6 +262,55 @@ struct WarpGroups {
 
 constexpr uint32_t kEncWarps = 4;
 
+// codag_fmt::RleV1Writer's bulk steps for a warp whose lanes all run the writer on one chunk
+struct WarpV1 {
+  static constexpr bool kBulk = true;
+  uint32_t lane_;
+  __device__ uint32_t lane() const { return lane_; }
+  __device__ uint32_t ballot(bool p) const { return __ballot_sync(FULL_MASK, p); }
+  __device__ uint32_t ffs(uint32_t m) const { return static_cast<uint32_t>(__ffs(m)); }
+  __device__ void sync() const { __syncwarp(); }
+  template <typename V>
+  __device__ V shfl(V v, int src) const {
+    if constexpr (sizeof(V) == 8) return static_cast<V>(__shfl_sync(FULL_MASK, static_cast<unsigned long long>(v), src));
+    else return static_cast<V>(__shfl_sync(FULL_MASK, static_cast<uint32_t>(v), src));
+  }
+  // the value of the lane below (lane 0 gets its own)
+  template <typename V>
+  __device__ V shfl_up(V v) const {
+    if constexpr (sizeof(V) == 8) return static_cast<V>(__shfl_up_sync(FULL_MASK, static_cast<unsigned long long>(v), 1));
+    else return static_cast<V>(__shfl_up_sync(FULL_MASK, static_cast<uint32_t>(v), 1));
+  }
+  // sum of v over the lanes below
+  __device__ uint32_t excl_sum(uint32_t v) const {
+    uint32_t s = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t o = __shfl_up_sync(FULL_MASK, s, d);
+      if (lane_ >= static_cast<uint32_t>(d)) s += o;
+    }
+    return s - v;
+  }
+};
+
+// RLE v1, one warp per chunk: every lane runs the writer on the same values (lane 0 writes its
+// single bytes); literal streams and runs going on are taken 32 values at a time (WarpV1)
+template <typename T>
+__global__ void __launch_bounds__(32 * kEncWarps) k_encode_rlev1_warp(const uint8_t* __restrict__ in, uint64_t in_bytes,
+                                                                     uint64_t chunk_bytes, uint64_t n,
+                                                                     uint8_t* __restrict__ scratch, uint64_t slot,
+                                                                     uint64_t* __restrict__ lens) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * kEncWarps + (threadIdx.x >> 5);
+  if (i >= n) return;  // the whole warp
+  WarpSink s{scratch + i * slot, slot, 0, lane};
+  using W = typename Wide<T>::T;
+  const PaddedChunk<W> get{in, in_bytes, i * chunk_bytes};
+  codag_fmt::RleV1Writer<T, WarpSink, WarpV1> w(s, WarpV1{lane});
+  w.encode([&](uint64_t j) { return static_cast<T>(get(j)); }, chunk_bytes / sizeof(T));
+  if (lane == 0) lens[i] = s.n > slot ? kOverflow : s.n;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(32 * kEncWarps) k_encode_rlev2_warp(const uint8_t* __restrict__ in, uint64_t in_bytes,
                                                                      uint64_t chunk_bytes, uint64_t n,
@@ -407,8 +426,8 @@ void launch_encode(const uint8_t* in, uint64_t in_bytes, uint64_t chunk, uint64_
     k_encode_rlev2_warp<T><<<static_cast<unsigned>((n + kEncWarps - 1) / kEncWarps), 32 * kEncWarps, 0, s>>>(
         in, in_bytes, chunk, n, scratch, slot, lens);
   } else {
-    k_encode_chunks<CODEC, T><<<static_cast<unsigned>((n + 31) / 32), 32, 0, s>>>(in, in_bytes, chunk, n, scratch, slot,
-                                                                                   lens);
+    k_encode_rlev1_warp<T><<<static_cast<unsigned>((n + kEncWarps - 1) / kEncWarps), 32 * kEncWarps, 0, s>>>(
+        in, in_bytes, chunk, n, scratch, slot, lens);
   }
 }
 

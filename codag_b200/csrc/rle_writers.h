@@ -35,10 +35,19 @@
 
 namespace codag_fmt {
 
-template <typename T, class Sink>
+// The RLE v1 writer's bulk steps: none when one thread runs the writer (host producers).  A warp
+// whose lanes all run the writer on the same values (the GPU encoder) supplies lane(), ballot(),
+// shuffles and an exclusive sum, and takes the values of a literal stream or of a run going on
+// many at a time (RleV1Writer::bulk).
+struct SerialV1 {
+  static constexpr bool kBulk = false;
+};
+
+template <typename T, class Sink, class G = SerialV1>
 class RleV1Writer {
  public:
   CODAG_HD explicit RleV1Writer(Sink& out) : out_(out) {}
+  CODAG_HD RleV1Writer(Sink& out, const G& g) : out_(out), g_(g) {}
 
   // n >= 2 values, value i read as get(i)
   template <class Get>
@@ -71,6 +80,13 @@ class RleV1Writer {
     held_++;
 
     for (; i < n; i++) {
+      if constexpr (G::kBulk) {
+        const uint32_t took = bulk(get, i, n);
+        if (took) {
+          i += took - 1;  // the loop's increment moves to the first value not taken
+          continue;
+        }
+      }
       if (lit_n_ == 127) close_literals();
       x = get(i);
 
@@ -180,6 +196,86 @@ class RleV1Writer {
   }
 
  private:
+  // Values i, i+1, ... (at most one per lane) that take the same steps as the value before them:
+  // in a run going on (three or more values, step in range), values that continue it, while the
+  // run stays below 130 values; in a literal stream (one value held), values whose step from the
+  // one before is out of range, each writing the value before it as a literal.  The steps are
+  // the per-value ones of encode() below, done for all taken values at once; returns the count
+  // (0: encode() takes value i).
+  template <class Get>
+  CODAG_HD uint32_t bulk(const Get& get, uint64_t i, uint64_t n) {
+    const uint32_t lane = g_.lane();
+    const uint64_t j = i + lane;
+    const bool in = j < n;
+    const T x = in ? static_cast<T>(get(j)) : T(0);
+    T before = g_.template shfl_up<T>(x);
+    if (lane == 0) before = prev_;
+    uint32_t take;
+    if (run_len_ >= 3 && in_run_) {
+      const uint32_t stop = g_.ballot(!(in && before + step_ == x));
+      take = stop ? g_.ffs(stop) - 1u : 32u;
+      const uint32_t room = 129u - run_len_;  // the value making 130 writes the run (encode())
+      if (take > room) take = room;
+      if (!take) return 0;
+      run_len_ = static_cast<uint16_t>(run_len_ + take);
+      held_ = static_cast<uint8_t>(held_ + take < 2 ? held_ + take : 2);
+    } else if (run_len_ == 1) {
+      const int64_t d = static_cast<int64_t>(x - before);
+      const uint32_t stop = g_.ballot(!(in && (d > 127 || d < -128)));
+      take = stop ? g_.ffs(stop) - 1u : 32u;
+      if (!take) return 0;
+      // literal k writes `before`; a group header goes before literal k when L0 + k is a multiple
+      // of 127 (at most once in 32 literals): a close of the full group and an open, or only an
+      // open when nothing was pending
+      const uint32_t l0 = lit_n_;
+      const uint32_t ev = l0 == 0 ? 0u : (127u - l0) % 127u;  // literal index of the header
+      const bool has_ev = ev < take;
+      const bool mine = lane < take;
+      const uint32_t hdr = (mine && has_ev && lane == ev) ? 1u : 0u;
+      uint32_t vlen = 0;
+      if (mine) {
+        T w = before;
+        do {
+          vlen++;
+          w = static_cast<T>(w >> 7);
+        } while (w != 0);
+      }
+      const uint32_t at = g_.excl_sum(hdr + vlen);
+      const uint32_t total = g_.template shfl<uint32_t>(at + hdr + vlen, 31);
+      if (has_ev && l0 != 0) out_.set(lit_hdr_, static_cast<uint8_t>(static_cast<int8_t>(-127)));
+      if (mine) {
+        uint32_t p = at;
+        if (hdr) out_.put_at(p++, 1);  // the placeholder open_literals(1) writes
+        T w = before;
+        do {
+          int8_t b = static_cast<int8_t>(w & 0x7F);
+          if ((w & (~0x7f)) != 0) b = static_cast<int8_t>(b | 0x80);
+          out_.put_at(p++, static_cast<uint8_t>(b));
+          w = static_cast<T>(w >> 7);
+        } while (w != 0);
+      }
+      if (has_ev) {
+        lit_hdr_ = out_.size() + g_.template shfl<uint32_t>(at, static_cast<int>(ev));
+        lit_n_ = static_cast<uint16_t>(take - ev);
+      } else {
+        lit_n_ = static_cast<uint16_t>(l0 + take);
+      }
+      out_.advance(total);
+      in_run_ = false;
+    } else {
+      return 0;
+    }
+    // the last two values taken become the history (push_hist per value)
+    const T last = g_.template shfl<T>(x, static_cast<int>(take - 1));
+    const T second = take >= 2 ? g_.template shfl<T>(x, static_cast<int>(take - 2)) : prev_;
+    head_ = static_cast<uint8_t>(head_ ^ (take & 1u));
+    hist_[head_ ^ 1] = last;
+    hist_[head_] = second;
+    prev_ = last;
+    g_.sync();
+    return take;
+  }
+
   CODAG_HD void put(uint8_t b) { out_.put(b); }
 
   // unsigned LEB128 in the element type's arithmetic (encoder.h:839-853)
@@ -209,6 +305,7 @@ class RleV1Writer {
   }
 
   Sink& out_;
+  G g_;
   T hist_[2] = {0, 0};
   uint8_t head_ = 0;
   uint8_t held_ = 0;

@@ -19,6 +19,16 @@ def _columns(native, codec, e):
     yield gen(CH // e, 400 + e, e)                                    # exactly one chunk
     yield rng.integers(0, 256, 2 * CH + 77, dtype=np.uint8)           # random bytes
     yield np.zeros(CH + 16, np.uint8)                                 # long zero runs
+    # runs around the 130-value run limit and literal bursts around the 127-literal group limit
+    parts = []
+    for k, ln in enumerate([128, 129, 130, 131, 260, 126, 127, 128, 254, 255, 3, 1, 2]):
+        if k < 5:
+            parts.append((np.arange(ln, dtype=np.uint64) * 3 + 1000 * k))
+        else:
+            parts.append(rng.integers(0, 1 << 62, ln, dtype=np.uint64) * 509)
+    vals = np.concatenate(parts * 8)
+    dt = {1: np.uint8, 2: np.uint16, 4: np.uint32, 8: np.uint64}[e]
+    yield vals.astype(dt).view(np.uint8)
 
 
 @pytest.mark.parametrize("codec", [0, 1], ids=["rlev1", "rlev2"])
