@@ -376,6 +376,46 @@ def measure_encode(workload: str, local: int, steps: int = 5) -> dict:
             "how": f"codag_compress_rlev{codec + 1}: one warp per chunk, scan, gather; input bytes per second"}
 
 
+def measure_transposed(local: int, steps: int = 10, read_unit: int = 1) -> dict:
+    """CODAG's transposed RLE v2 layout (32 interleaved substreams per chunk) of the RLE v2
+    workload's 1 GiB int64 column, written by the host producer and decoded resident in HBM by
+    codag_decompress_rlev2_transposed: decompressed GB/s, its HBM roofline, byte equality."""
+    import torch
+    from codag_b200 import api, native as nat
+    f = make_file("rlev2", 0)
+    col = f["col"]
+    comp, off, ln = nat.encode_rlev2_transposed(col, CH, 8, read_unit)
+    n = ln.size // 32
+    dev = torch.device("cuda", local)
+    d_comp = torch.from_numpy(comp).to(dev)
+    d_off = torch.from_numpy(off[:n].view(np.int64)).to(dev)
+    d_len = torch.from_numpy(ln.view(np.int64)).to(dev)
+    out = torch.empty(col.nbytes, dtype=torch.uint8, device=dev)
+    st = torch.zeros(n, dtype=torch.int32, device=dev)
+    run = lambda: api.decompress_rlev2_transposed(d_comp, d_off, d_len, CH, 8, read_unit, out, col.nbytes, st)
+    for _ in range(3):
+        run()
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(steps):
+        run()
+    t1.record()
+    torch.cuda.synchronize()
+    dt = t0.elapsed_time(t1) / 1e3 / steps
+    ok = int((st != 0).sum().item()) == 0 and bool(torch.equal(out, torch.from_numpy(col.view(np.uint8)).to(dev)))
+    peak, peak_kind = peaks()
+    alg = int(comp.size) + int(col.nbytes)
+    del d_comp, d_off, d_len, out, st
+    torch.cuda.empty_cache()
+    return {"workload": f"transposed RLE v2 (read unit {read_unit}), {WORKLOADS['rlev2']['desc']}",
+            "value": round(col.nbytes / dt / 1e9, 2), "unit": "GB/s", "ms_per_step": round(dt * 1e3, 4),
+            "bit_exact": ok, "roofline": {"bound": "hbm", "achieved": round(alg / dt / 1e9, 1), "peak": peak,
+                                          "unit": "GB/s", "frac": round(alg / dt / 1e9 / peak, 4), "traffic": None,
+                                          "peak_kind": peak_kind, "kernel": "k_rlev2_transposed<8>",
+                                          "alg_bytes_per_launch": alg}}
+
+
 def _summary(line: dict) -> dict:
     """The figures of a per-codec line kept under the headline's `configs`."""
     keep = ("value", "unit", "ms_per_step", "bit_exact", "e2e", "roofline", "cpu_baseline", "clocks")
@@ -442,6 +482,7 @@ def main():
                                                          clocks_on=False))
                 configs["encode_rlev2"] = measure_encode("rlev2", local)
                 configs["encode_rlev1"] = measure_encode("rlev1x128", local)
+                configs["rlev2_transposed"] = measure_transposed(local)
                 configs["serving"] = bench_serving.short_sweep(args, local)
                 line["configs"] = configs
                 line["configs_note"] = ("per-codec configurations and a short serving sweep, timed in the same run "
