@@ -413,7 +413,7 @@ def measure_transposed(local: int, steps: int = 10, read_unit: int = 1) -> dict:
             "bit_exact": ok, "roofline": {"bound": "hbm", "achieved": round(alg / dt / 1e9, 1), "peak": peak,
                                           "unit": "GB/s", "frac": round(alg / dt / 1e9 / peak, 4), "traffic": None,
                                           "peak_kind": peak_kind, "kernel": "k_rlev2_transposed<8>",
-                                          "alg_bytes_per_launch": alg}}
+                                          "alg_bytes_per_launch": alg, "launch_ms": round(dt * 1e3, 4)}}
 
 
 def _summary(line: dict) -> dict:
