@@ -5,11 +5,14 @@
 // the substreams in 4-byte words: word w of every substream longer than 4w, in substream
 // order, then word w+1.  CODAG decodes it with one lane per substream fed by a reader warp
 // through spin queues (include/rlev2/decoder_new.h:375-632, 1193-1230).  Here one warp
-// decodes a chunk with no queue: the warp first tabulates, per word index w, the mask of
-// substreams that still have a word w and the number of words before row w (shared memory),
-// so lane t finds its word w at row_start[w] + popc(mask[w] & lanes below t) by itself; then
-// every lane decodes its own substream and writes its values straight to their interleaved
-// places in global memory.  Header semantics are CODAG's (the oracle's restatement of
+// decodes a chunk with no queue.  The set of substreams that still have a word w only shrinks
+// as w grows, so it changes at most 32 times: the warp tabulates those segments of rows (first
+// and last row, the mask of substreams present, the words before the segment; at most 32
+// entries, 512 bytes of shared memory per warp), and lane t finds its word w at
+// start + (w - first row) * popc(mask) + popc(mask & lanes below t) by itself.  Then every
+// lane decodes its own substream and writes its values straight to their interleaved places
+// in global memory.  The small table leaves occupancy to the registers, so many chunks' lanes
+// wait on their word loads at once.  Header semantics are CODAG's (the oracle's restatement of
 // decoder_new.h:1000-1184, quirks included: the uint8_t run length, the 32-bit patch mask, the
 // arithmetic-shift zigzag and the DELTA direction taken from the base delta).
 #include <cuda_runtime.h>
@@ -27,14 +30,23 @@ __device__ __forceinline__ uint64_t shl64(uint64_t v, uint32_t s) { return s >= 
 __device__ __forceinline__ uint64_t shr64(uint64_t v, uint32_t s) { return s >= 64 ? 0ull : v >> s; }
 
 // bytes of one lane's substream, read word by word from the interleaved region
+// row segments of one chunk (shared memory): rows lo[s] <= w < hi[s] hold a word of exactly the
+// substreams in mask[s], and words[s] words of the region come before row lo[s]
+struct Segments {
+  uint32_t hi[32], lo[32], mask[32], words[32];
+};
+
+constexpr uint32_t kWarps = 4;  // chunks (warps) per block
+
 struct LaneReader {
   const uint32_t* region;  // the chunk's region (128-byte aligned)
-  const uint32_t* mask;    // shared: substreams with a word at each row
-  const uint32_t* start;   // shared: words before each row
+  const Segments* seg;
+  uint32_t total;          // words in the region
   uint32_t lt;             // lanes below this one
   uint32_t len;            // substream bytes
   uint32_t p;              // next byte
   uint32_t cw, cv;         // cached word index and value
+  uint32_t s;              // segment of cw (rows only grow, so it only moves forward)
   bool bad;
 
   __device__ __forceinline__ uint32_t byte() {
@@ -45,7 +57,15 @@ struct LaneReader {
     const uint32_t w = p >> 2;
     if (w != cw) {
       cw = w;
-      cv = __ldg(region + start[w] + __popc(mask[w] & lt));
+      // w < this substream's word count <= the last segment's hi, so the walk stays in the table
+      while (w >= seg->hi[s]) s++;
+      const uint32_t m = seg->mask[s];
+      const uint32_t at = seg->words[s] + (w - seg->lo[s]) * __popc(m) + __popc(m & lt);
+      if (at >= total) {
+        bad = true;
+        return 0;
+      }
+      cv = __ldg(region + at);
     }
     return (cv >> (8u * (p++ & 3u))) & 0xffu;
   }
@@ -77,6 +97,7 @@ struct LaneOut {
   T* chunk;
   uint32_t t, ru, cap, store;  // cap: values per substream; store: elements of the chunk to store
   uint32_t n;
+  uint32_t e, j;  // element of value n, and n % ru (stepped without a division)
   bool over;
   __device__ __forceinline__ uint32_t elem(uint32_t k) const { return t * ru + (k / ru) * 32u * ru + k % ru; }
   __device__ __forceinline__ void put(uint64_t v) {
@@ -84,8 +105,14 @@ struct LaneOut {
       over = true;
       return;
     }
-    const uint32_t e = elem(n++);
     if (e < store) chunk[e] = static_cast<T>(v);
+    n++;
+    if (++j == ru) {  // next group of ru values, 32 * ru elements on
+      j = 0;
+      e += 31u * ru + 1u;
+    } else {
+      e++;
+    }
   }
   __device__ __forceinline__ uint64_t get(uint32_t k) const {
     const uint32_t e = elem(k);
@@ -109,63 +136,24 @@ __device__ __forceinline__ uint64_t uvarint(LaneReader& r) {
   return v;
 }
 
+// One lane's substream as a state machine that yields one value per pass: a lane whose run
+// ends reads its next header while the other lanes go on with theirs, so the warp's lanes
+// meet again after every value instead of waiting for the longest run among them.
+enum : uint32_t { kNone, kRepeat, kDirect, kDeltaBits, kDeltaFixed, kPatched };
+
 template <typename T>
 __device__ int decode_substream(LaneReader& r, LaneOut<T>& o) {
   constexpr uint64_t M = sizeof(T) == 8 ? ~0ull : ((1ull << (8 * sizeof(T))) - 1ull);
-  while (r.p < r.len) {
-    const uint32_t first = r.byte();
-    switch (first & 0xC0u) {
-      case 0x00: {  // SHORT_REPEAT (decoder_new.h:1004-1014)
-        uint32_t nb = ((first >> 3) & 7u) + 1u, cnt = (first & 7u) + 3u;
-        uint64_t v = 0;
-        while (nb-- > 0) v |= shl64(r.byte(), nb * 8u);
-        while (cnt-- > 0) o.put(v & M);
-      } break;
-      case 0x40: {  // DIRECT (decoder_new.h:1015-1043)
-        const uint32_t fbw = v2_width((first >> 1) & 0x1fu);
-        uint8_t len = static_cast<uint8_t>((((first & 1u) << 8) | r.byte()) + 1u);
-        HeaderBits b{0, 0};
-        while (len-- > 0) o.put(b.read(r, fbw) & M);
-      } break;
-      case 0xC0: {  // DELTA (decoder_new.h:1044-1091)
-        const uint32_t enc = (first >> 1) & 0x1fu, fbw = v2_width(enc);
-        uint8_t len = static_cast<uint8_t>((((first & 1u) << 8) | r.byte()) + 1u);
-        uint64_t base = uvarint(r) & M;
-        const int64_t u = static_cast<int64_t>(uvarint(r));
-        const uint64_t bd = static_cast<uint64_t>((u >> 1) ^ -(u & 1)) & M;  // arithmetic shift (:990)
-        o.put(base);
-        base = (base + bd) & M;
-        o.put(base);
-        len = static_cast<uint8_t>(len - 2);
-        const bool plus = bd > 0;  // multiplier = base_delta > 0 ? 1 : -1 on the unsigned type (:1057)
-        if (enc != 0) {
-          HeaderBits b{0, 0};
-          while (len-- > 0) {
-            const uint64_t d = b.read(r, fbw) & M;
-            base = (plus ? base + d : base - d) & M;
-            o.put(base);
-          }
-        } else {
-          while (len-- > 0) {
-            base = (base + bd) & M;
-            o.put(base);
-          }
-        }
-      } break;
-      default: {  // PATCHED_BASE (decoder_new.h:1092-1183)
-        const uint32_t fbw = v2_width((first >> 1) & 0x1fu);
-        uint8_t len = static_cast<uint8_t>((((first & 1u) << 8) | r.byte()) + 1u);
-        const uint32_t third = r.byte(), fourth = r.byte();
-        uint32_t bw = ((third >> 5) & 7u) + 1u;
-        const uint32_t pw = v2_width(third & 0x1fu), pgw = ((fourth >> 5) & 7u) + 1u;
-        uint32_t pll = fourth & 0x1fu;
-        const uint64_t pmask = pw >= 32 ? 0xFFFFFFFFull : ((1ull << pw) - 1ull);  // 32-bit mask (:1103)
-        const uint32_t base_out = o.n;
-        uint64_t base = 0;
-        while (bw-- > 0) base |= shl64(r.byte(), bw * 8u);
-        HeaderBits b{0, 0};
-        while (len-- > 0) o.put((b.read(r, fbw) + base) & M);
+  uint32_t mode = kNone, rem = 0, fbw = 0;
+  uint64_t v = 0, bd = 0;  // repeat: the value; delta: running value and base delta; patched: base
+  bool plus = false;
+  uint32_t pw = 0, pgw = 0, pll = 0, base_out = 0;  // patched: patch width, gap width, list length
+  HeaderBits b{0, 0};
+  for (;;) {
+    if (rem == 0) {
+      if (mode == kPatched) {  // the run's values are out: patch them (decoder_new.h:1166-1183)
         if (pw + pgw > 64) return CODAG_ECORRUPT;
+        const uint64_t pmask = pw >= 32 ? 0xFFFFFFFFull : ((1ull << pw) - 1ull);  // 32-bit mask (:1103)
         const uint32_t cfb = v2_closest(pw + pgw);
         b = HeaderBits{0, 0};
         uint64_t gap = 0;
@@ -175,11 +163,83 @@ __device__ int decode_substream(LaneReader& r, LaneOut<T>& o) {
           const uint64_t idx = base_out + gap;
           if (r.bad || idx >= o.n || o.over) return CODAG_ECORRUPT;
           const uint64_t patch = shl64((ent & pmask) & M, fbw) & M;
-          const uint64_t v = o.get(static_cast<uint32_t>(idx));
-          o.set(static_cast<uint32_t>(idx), ((((v - base) & M) | patch) + base) & M);
+          const uint64_t x = o.get(static_cast<uint32_t>(idx));
+          o.set(static_cast<uint32_t>(idx), ((((x - v) & M) | patch) + v) & M);
         }
-      } break;
+        if (r.bad || o.over) return CODAG_ECORRUPT;
+      }
+      mode = kNone;
+      if (r.p >= r.len) break;
+      const uint32_t first = r.byte();
+      b = HeaderBits{0, 0};
+      switch (first & 0xC0u) {
+        case 0x00: {  // SHORT_REPEAT (decoder_new.h:1004-1014)
+          uint32_t nb = ((first >> 3) & 7u) + 1u;
+          rem = (first & 7u) + 3u;
+          v = 0;
+          while (nb-- > 0) v |= shl64(r.byte(), nb * 8u);
+          v &= M;
+          mode = kRepeat;
+        } break;
+        case 0x40:  // DIRECT (decoder_new.h:1015-1043)
+          fbw = v2_width((first >> 1) & 0x1fu);
+          rem = static_cast<uint8_t>((((first & 1u) << 8) | r.byte()) + 1u);  // a uint8_t length (:1018)
+          mode = kDirect;
+          break;
+        case 0xC0: {  // DELTA (decoder_new.h:1044-1091)
+          const uint32_t enc = (first >> 1) & 0x1fu;
+          fbw = v2_width(enc);
+          const uint8_t len = static_cast<uint8_t>((((first & 1u) << 8) | r.byte()) + 1u);
+          v = uvarint(r) & M;
+          const int64_t u = static_cast<int64_t>(uvarint(r));
+          bd = static_cast<uint64_t>((u >> 1) ^ -(u & 1)) & M;  // arithmetic shift (:990)
+          o.put(v);
+          v = (v + bd) & M;
+          o.put(v);
+          rem = static_cast<uint8_t>(len - 2);
+          plus = bd > 0;  // multiplier = base_delta > 0 ? 1 : -1 on the unsigned type (:1057)
+          mode = enc != 0 ? kDeltaBits : kDeltaFixed;
+        } break;
+        default: {  // PATCHED_BASE (decoder_new.h:1092-1165)
+          fbw = v2_width((first >> 1) & 0x1fu);
+          rem = static_cast<uint8_t>((((first & 1u) << 8) | r.byte()) + 1u);
+          const uint32_t third = r.byte(), fourth = r.byte();
+          uint32_t bw = ((third >> 5) & 7u) + 1u;
+          pw = v2_width(third & 0x1fu);
+          pgw = ((fourth >> 5) & 7u) + 1u;
+          pll = fourth & 0x1fu;
+          base_out = o.n;
+          v = 0;
+          while (bw-- > 0) v |= shl64(r.byte(), bw * 8u);
+          mode = kPatched;
+        } break;
+      }
+      if (r.bad || o.over) return CODAG_ECORRUPT;
+      if (rem == 0) continue;
     }
+    uint64_t x;
+    switch (mode) {
+      case kRepeat:
+        x = v;
+        break;
+      case kDirect:
+        x = b.read(r, fbw) & M;
+        break;
+      case kDeltaBits: {
+        const uint64_t d = b.read(r, fbw) & M;
+        v = (plus ? v + d : v - d) & M;
+        x = v;
+      } break;
+      case kDeltaFixed:
+        v = (v + bd) & M;
+        x = v;
+        break;
+      default:  // kPatched
+        x = (b.read(r, fbw) + v) & M;
+        break;
+    }
+    o.put(x);
+    rem--;
     if (r.bad || o.over) return CODAG_ECORRUPT;
   }
   return CODAG_OK;
@@ -193,18 +253,16 @@ __device__ __forceinline__ uint32_t needed(uint32_t t, uint32_t ru, uint32_t sto
 }
 
 template <typename T>
-__global__ void __launch_bounds__(128) k_rlev2_transposed(const uint8_t* __restrict__ comp, uint64_t comp_bytes,
-                                                          const uint64_t* __restrict__ blk_off,
-                                                          const uint64_t* __restrict__ col_len, uint64_t n_chunks,
-                                                          uint64_t chunk_bytes, uint32_t ru, uint8_t* __restrict__ out,
-                                                          uint64_t out_bytes, int32_t* __restrict__ status,
-                                                          uint32_t max_words) {
-  extern __shared__ uint32_t tabs[];
+__global__ void __launch_bounds__(32 * kWarps)
+    k_rlev2_transposed(const uint8_t* __restrict__ comp, uint64_t comp_bytes, const uint64_t* __restrict__ blk_off,
+                       const uint64_t* __restrict__ col_len, uint64_t n_chunks, uint64_t chunk_bytes, uint32_t ru,
+                       uint8_t* __restrict__ out, uint64_t out_bytes, int32_t* __restrict__ status,
+                       uint32_t max_words) {
+  __shared__ Segments segs[kWarps];
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint64_t c = static_cast<uint64_t>(blockIdx.x) * (blockDim.x >> 5) + warp;
   if (c >= n_chunks) return;
-  uint32_t* mask = tabs + warp * 2u * max_words;
-  uint32_t* start = mask + max_words;
+  Segments* seg = segs + warp;
   const uint64_t len64 = col_len[32 * c + lane];
   const uint32_t words = static_cast<uint32_t>(len64 < (1ull << 34) ? (len64 + 3) / 4 : 0xffffffffu);
   const uint32_t maxw = __reduce_max_sync(FULL, words);
@@ -217,20 +275,25 @@ __global__ void __launch_bounds__(128) k_rlev2_transposed(const uint8_t* __restr
                                                              ? out_bytes - c * chunk_bytes : chunk_bytes) : 0;
   const uint32_t store = static_cast<uint32_t>(store_b / sizeof(T));
   if (st == CODAG_OK) {
-    uint32_t run = 0;
-    for (uint32_t w = 0; w < maxw; w++) {  // row w: substreams with a word w, words before it
-      const uint32_t m = __ballot_sync(FULL, words > w);
+    // one segment per distinct word count: each pass drops at least one substream, so at most 32
+    uint32_t run = 0, row = 0, ns = 0;
+    for (uint32_t m = __ballot_sync(FULL, words > 0); m; m = __ballot_sync(FULL, words > row)) {
+      const uint32_t nxt = __reduce_min_sync(FULL, words > row ? words : 0xffffffffu);
       if (lane == 0) {
-        mask[w] = m;
-        start[w] = run;
+        seg->hi[ns] = nxt;
+        seg->lo[ns] = row;
+        seg->mask[ns] = m;
+        seg->words[ns] = run;
       }
-      run += __popc(m);
+      run += (nxt - row) * __popc(m);
+      row = nxt;
+      ns++;
     }
     __syncwarp();
-    LaneReader r{reinterpret_cast<const uint32_t*>(comp + off), mask, start, (1u << lane) - 1u,
-                 static_cast<uint32_t>(len64), 0, 0xffffffffu, 0, false};
+    LaneReader r{reinterpret_cast<const uint32_t*>(comp + off), seg, run, (1u << lane) - 1u,
+                 static_cast<uint32_t>(len64), 0, 0xffffffffu, 0, 0, false};
     LaneOut<T> o{reinterpret_cast<T*>(out) + base_e, lane, ru,
-                 static_cast<uint32_t>(chunk_bytes / sizeof(T) / 32), store, 0, false};
+                 static_cast<uint32_t>(chunk_bytes / sizeof(T) / 32), store, 0, lane * ru, 0, false};
     int s = decode_substream<T>(r, o);
     if (s == CODAG_OK && o.n < needed(lane, ru, store)) s = CODAG_ECORRUPT;
     st = __reduce_max_sync(FULL, static_cast<uint32_t>(s));
@@ -246,15 +309,11 @@ codag_status launch(const uint8_t* comp, uint64_t comp_bytes, const uint64_t* bl
                     cudaStream_t s) {
   // a substream is at most about twice its share of the chunk (the encoders' bound), in words
   const uint32_t max_words = static_cast<uint32_t>((chunk / 32 * 2 + 1024) / 4);
-  constexpr uint32_t kWarps = 4;
-  const uint32_t smem = kWarps * 2u * max_words * 4u;
-  auto kern = k_rlev2_transposed<T>;
-  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) != cudaSuccess)
-    return CODAG_ECUDA;
   const uint64_t grid = (n + kWarps - 1) / kWarps;
   if (grid > 0x7fffffffull) return CODAG_EINVAL;
-  kern<<<static_cast<unsigned>(grid), 32 * kWarps, smem, s>>>(comp, comp_bytes, blk_off, col_len, n, chunk, ru, out,
-                                                              out_bytes, status, max_words);
+  k_rlev2_transposed<T><<<static_cast<unsigned>(grid), 32 * kWarps, 0, s>>>(comp, comp_bytes, blk_off, col_len, n,
+                                                                            chunk, ru, out, out_bytes, status,
+                                                                            max_words);
   return cudaGetLastError() == cudaSuccess ? CODAG_OK : CODAG_ECUDA;
 }
 
