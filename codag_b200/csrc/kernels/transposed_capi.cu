@@ -49,6 +49,19 @@ struct LaneReader {
   uint32_t s;              // segment of cw (rows only grow, so it only moves forward)
   bool bad;
 
+  // where word w of this substream sits in the region; w < its word count <= the last
+  // segment's hi keeps the walk inside the table, and the region has `total` words
+  __device__ __forceinline__ uint32_t start(uint32_t w) {
+    while (w >= seg->hi[s]) s++;
+    const uint32_t m = seg->mask[s];
+    const uint32_t at = seg->words[s] + (w - seg->lo[s]) * __popc(m) + __popc(m & lt);
+    if (at >= total) {
+      bad = true;
+      return 0;
+    }
+    return at;
+  }
+
   __device__ __forceinline__ uint32_t byte() {
     if (p >= len) {
       bad = true;
@@ -57,37 +70,49 @@ struct LaneReader {
     const uint32_t w = p >> 2;
     if (w != cw) {
       cw = w;
-      // w < this substream's word count <= the last segment's hi, so the walk stays in the table
-      while (w >= seg->hi[s]) s++;
-      const uint32_t m = seg->mask[s];
-      const uint32_t at = seg->words[s] + (w - seg->lo[s]) * __popc(m) + __popc(m & lt);
-      if (at >= total) {
-        bad = true;
-        return 0;
-      }
-      cv = __ldg(region + at);
+      cv = __ldg(region + start(w));
     }
     return (cv >> (8u * (p++ & 3u))) & 0xffu;
   }
-};
 
-// MSB-first bits local to one header (decoder_new.h:1024-1040)
-struct HeaderBits {
-  uint32_t cur, left;
-  __device__ __forceinline__ uint64_t read(LaneReader& r, uint32_t n) {
-    uint64_t v = 0;
-    while (n > left) {
-      v = shl64(v, left) | (cur & ((1u << left) - 1u));
-      n -= left;
-      cur = r.byte();
-      left = 8;
+  // the next k (1..8) bytes as one big-endian number, a word's worth of bytes per step
+  __device__ __forceinline__ uint64_t take(uint32_t k) {
+    if (k > len - p) {
+      bad = true;
+      return 0;
     }
-    if (n) {
-      v = shl64(v, n);
-      left -= n;
-      v |= (cur >> left) & ((1u << n) - 1u);
+    uint64_t v = 0;
+    while (k) {
+      const uint32_t w = p >> 2;
+      if (w != cw) {
+        cw = w;
+        cv = __ldg(region + start(w));
+      }
+      const uint32_t o = p & 3u, m = k < 4u - o ? k : 4u - o;
+      const uint32_t be = __byte_perm(cv, 0u, 0x0123u) << (8u * o);  // stream bytes o.. at the top
+      v = (v << (8u * m)) | (be >> (32u - 8u * m));
+      p += m;
+      k -= m;
     }
     return v;
+  }
+};
+
+// MSB-first bits local to one header (decoder_new.h:1024-1040): `cur` holds the last byte
+// taken, its low `left` bits not yet read
+struct HeaderBits {
+  uint32_t cur, left;
+  __device__ __forceinline__ uint64_t read(LaneReader& r, uint32_t n) {  // n <= 64
+    if (n <= left) {
+      left -= n;
+      return (cur >> left) & ((1u << n) - 1u);
+    }
+    const uint32_t need = n - left, k = (need + 7u) >> 3;
+    const uint64_t hi = cur & ((1u << left) - 1u);
+    const uint64_t lo = r.take(k);
+    left = 8u * k - need;
+    cur = static_cast<uint32_t>(lo) & 0xffu;
+    return shl64(hi, need) | (lo >> left);
   }
 };
 
