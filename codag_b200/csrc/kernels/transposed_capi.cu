@@ -163,20 +163,22 @@ __device__ __forceinline__ uint64_t uvarint(LaneReader& r) {
 
 // One lane's substream as a state machine that yields one value per pass: a lane whose run
 // ends reads its next header while the other lanes go on with theirs, so the warp's lanes
-// meet again after every value instead of waiting for the longest run among them.
-enum : uint32_t { kNone, kRepeat, kDirect, kDeltaBits, kDeltaFixed, kPatched };
+// meet again after every value instead of waiting for the longest run among them.  Every run
+// kind yields its next value by one step, x = v + d or v - d (v kept as x for the kinds that
+// accumulate), d being the run's next bit field or a constant, so the only fork inside the
+// step is whether the lane reads bits.
 
 template <typename T>
 __device__ int decode_substream(LaneReader& r, LaneOut<T>& o) {
   constexpr uint64_t M = sizeof(T) == 8 ? ~0ull : ((1ull << (8 * sizeof(T))) - 1ull);
-  uint32_t mode = kNone, rem = 0, fbw = 0;
+  uint32_t rem = 0, fbw = 0;
   uint64_t v = 0, bd = 0;  // repeat: the value; delta: running value and base delta; patched: base
-  bool plus = false;
+  bool bits = false, acc = false, sub = false, patched = false;
   uint32_t pw = 0, pgw = 0, pll = 0, base_out = 0;  // patched: patch width, gap width, list length
   HeaderBits b{0, 0};
   for (;;) {
     if (rem == 0) {
-      if (mode == kPatched) {  // the run's values are out: patch them (decoder_new.h:1166-1183)
+      if (patched) {  // the run's values are out: patch them (decoder_new.h:1166-1183)
         if (pw + pgw > 64) return CODAG_ECORRUPT;
         const uint64_t pmask = pw >= 32 ? 0xFFFFFFFFull : ((1ull << pw) - 1ull);  // 32-bit mask (:1103)
         const uint32_t cfb = v2_closest(pw + pgw);
@@ -193,23 +195,24 @@ __device__ int decode_substream(LaneReader& r, LaneOut<T>& o) {
         }
         if (r.bad || o.over) return CODAG_ECORRUPT;
       }
-      mode = kNone;
+      patched = false;
       if (r.p >= r.len) break;
       const uint32_t first = r.byte();
       b = HeaderBits{0, 0};
       switch (first & 0xC0u) {
         case 0x00: {  // SHORT_REPEAT (decoder_new.h:1004-1014)
-          uint32_t nb = ((first >> 3) & 7u) + 1u;
           rem = (first & 7u) + 3u;
-          v = 0;
-          while (nb-- > 0) v |= shl64(r.byte(), nb * 8u);
-          v &= M;
-          mode = kRepeat;
+          v = r.take(((first >> 3) & 7u) + 1u) & M;  // a big-endian value of 1..8 bytes
+          bd = 0;
+          bits = sub = false;
+          acc = true;
         } break;
         case 0x40:  // DIRECT (decoder_new.h:1015-1043)
           fbw = v2_width((first >> 1) & 0x1fu);
           rem = static_cast<uint8_t>((((first & 1u) << 8) | r.byte()) + 1u);  // a uint8_t length (:1018)
-          mode = kDirect;
+          v = 0;
+          bits = true;
+          acc = sub = false;
           break;
         case 0xC0: {  // DELTA (decoder_new.h:1044-1091)
           const uint32_t enc = (first >> 1) & 0x1fu;
@@ -222,47 +225,29 @@ __device__ int decode_substream(LaneReader& r, LaneOut<T>& o) {
           v = (v + bd) & M;
           o.put(v);
           rem = static_cast<uint8_t>(len - 2);
-          plus = bd > 0;  // multiplier = base_delta > 0 ? 1 : -1 on the unsigned type (:1057)
-          mode = enc != 0 ? kDeltaBits : kDeltaFixed;
+          bits = enc != 0;  // else every step adds the base delta
+          sub = bits && bd == 0;  // multiplier = base_delta > 0 ? 1 : -1 on the unsigned type (:1057)
+          acc = true;
         } break;
         default: {  // PATCHED_BASE (decoder_new.h:1092-1165)
           fbw = v2_width((first >> 1) & 0x1fu);
           rem = static_cast<uint8_t>((((first & 1u) << 8) | r.byte()) + 1u);
-          const uint32_t third = r.byte(), fourth = r.byte();
-          uint32_t bw = ((third >> 5) & 7u) + 1u;
-          pw = v2_width(third & 0x1fu);
-          pgw = ((fourth >> 5) & 7u) + 1u;
-          pll = fourth & 0x1fu;
+          const uint32_t h = static_cast<uint32_t>(r.take(2));  // third and fourth header bytes
+          pw = v2_width((h >> 8) & 0x1fu);
+          pgw = ((h >> 5) & 7u) + 1u;
+          pll = h & 0x1fu;
           base_out = o.n;
-          v = 0;
-          while (bw-- > 0) v |= shl64(r.byte(), bw * 8u);
-          mode = kPatched;
+          v = r.take(((h >> 13) & 7u) + 1u);  // the big-endian base, 1..8 bytes
+          bits = patched = true;
+          acc = sub = false;
         } break;
       }
       if (r.bad || o.over) return CODAG_ECORRUPT;
       if (rem == 0) continue;
     }
-    uint64_t x;
-    switch (mode) {
-      case kRepeat:
-        x = v;
-        break;
-      case kDirect:
-        x = b.read(r, fbw) & M;
-        break;
-      case kDeltaBits: {
-        const uint64_t d = b.read(r, fbw) & M;
-        v = (plus ? v + d : v - d) & M;
-        x = v;
-      } break;
-      case kDeltaFixed:
-        v = (v + bd) & M;
-        x = v;
-        break;
-      default:  // kPatched
-        x = (b.read(r, fbw) + v) & M;
-        break;
-    }
+    const uint64_t d = bits ? b.read(r, fbw) & M : bd;
+    const uint64_t x = (sub ? v - d : v + d) & M;
+    if (acc) v = x;
     o.put(x);
     rem--;
     if (r.bad || o.over) return CODAG_ECORRUPT;
