@@ -123,3 +123,48 @@ def test_cuda_round_trip_of_writer(cuda, native, e, ru):
     for c in np.nonzero(ok)[0]:
         hi = min((c + 1) * CH, col.size)
         assert np.array_equal(got[c * CH:hi], col[c * CH:hi]), c
+
+
+def _damaged(native, seed):
+    """A writer's file of 8 int64 chunks, damaged: a byte flipped in chunks 1, 3 and 5, a
+    substream cut by 3 bytes in chunk 2, one emptied in chunk 6, and chunk 7 claiming a
+    substream far longer than the file (chunks 0 and 4 intact)."""
+    col = native.gen_rlev2_column(8 * CH // 8, seed, 8)
+    comp, off, ln = native.encode_rlev2_transposed(col, CH, 8, 1)
+    comp, ln = comp.copy(), ln.astype(np.uint64).copy()
+    rng = np.random.default_rng(seed)
+    for c in (1, 3, 5):
+        at = int(off[c]) + int(rng.integers(0, int(off[c + 1] - off[c])))
+        comp[at] ^= np.uint8(1 << int(rng.integers(0, 8)))
+    ln[32 * 2 + 5] -= 3
+    ln[32 * 6 + 17] = 0
+    ln[32 * 7 + 9] = 1 << 40
+    return col, {"comp": comp, "blk_off": off, "col_len": ln, "elem": 8, "read_unit": 1}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", [41, 42, 43])
+def test_cuda_decoder_on_damaged_files(cuda, native, oracle, seed):
+    """Damaged chunks decode as the oracle decodes them: a chunk the kernel passes, the oracle
+    passes with the same bytes, a chunk the oracle rejects the kernel rejects, a substream
+    longer than the file is ECORRUPT, and the intact chunks still decode to the column."""
+    from codag_b200 import api
+    col, g = _damaged(native, seed)
+    n = 8
+    t = lambda a: cuda.from_numpy(np.ascontiguousarray(a).astype(np.uint64).view(np.int64)).to("cuda")
+    out = cuda.zeros(n * CH, dtype=cuda.uint8, device="cuda")
+    st = cuda.full((n,), -1, dtype=cuda.int32, device="cuda")
+    api.decompress_rlev2_transposed(cuda.from_numpy(g["comp"]).to("cuda"), t(g["blk_off"][:n]), t(g["col_len"]),
+                                    CH, 8, 1, out, col.nbytes, st)
+    cuda.cuda.synchronize()
+    got, gst = out.cpu().numpy(), st.cpu().numpy()
+    src = col.view(np.uint8)
+    for c in (0, 4):
+        assert gst[c] == 0 and np.array_equal(got[c * CH:(c + 1) * CH], src[c * CH:(c + 1) * CH]), c
+    assert gst[7] == 2  # CODAG_ECORRUPT
+    for c in range(7):
+        ost, want = _oracle_chunk(oracle, g, c)
+        if gst[c] == 0:
+            assert ost == 0 and np.array_equal(got[c * CH:(c + 1) * CH], want), c
+        if ost != 0:
+            assert gst[c] != 0, c
