@@ -612,7 +612,7 @@ class RleV2Writer {
   }
   CODAG_HD void put_svarint(int64_t val) { put_uvarint((val << 1) ^ (val >> 63)); }
 
-  CODAG_HD void write_short_repeat() {
+  CODAG_HD_CALL void write_short_repeat() {
     const uint64_t val = lit_[0];
     const uint8_t nbytes = static_cast<uint8_t>((closest_width(val) - 1) / 8 + 1);
     put(static_cast<uint8_t>(((nbytes - 1) << 3) | (fix_ - kMinRepeat)));
@@ -622,7 +622,7 @@ class RleV2Writer {
     var_ = 0;
   }
 
-  CODAG_HD void write_direct() {
+  CODAG_HD_CALL void write_direct() {
     uint8_t hist[32];
     const uint64_t* l = lit_;
     const auto lit = [l](uint32_t i) { return l[i]; };
@@ -642,7 +642,7 @@ class RleV2Writer {
     nlit_ = 0;
   }
 
-  CODAG_HD void write_delta() {
+  CODAG_HD_CALL void write_delta() {
     uint16_t len;
     uint8_t enc = 0;
     uint8_t bits = v2_closest_aligned(delta_bits_);
@@ -673,7 +673,7 @@ class RleV2Writer {
     var_ = 0;
   }
 
-  CODAG_HD void write_patched(uint64_t lit_min, uint8_t b95, uint8_t b100) {
+  CODAG_HD_CALL void write_patched(uint64_t lit_min, uint8_t b95, uint8_t b100) {
     // patch list (preparePatchedBlob1, encoder.h:182-268); a group holds at most 128 values, so
     // every gap is below 256 and each patch takes one list entry
     int64_t mask = static_cast<int64_t>((static_cast<uint64_t>(1) << b95) - 1);
@@ -712,7 +712,7 @@ class RleV2Writer {
   }
 
   // determineEncoding (encoder.h:270-387)
-  CODAG_HD void choose_encoding() {
+  CODAG_HD_CALL void choose_encoding() {
     if (nlit_ <= static_cast<uint32_t>(kMinRepeat)) {
       write_direct();
       return;

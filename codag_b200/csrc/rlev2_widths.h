@@ -10,8 +10,12 @@
 
 #if defined(__CUDACC__)
 #define CODAG_HD __host__ __device__ __forceinline__
+// a large step called from many places, kept as one copy so that a warp's loop fits the
+// instruction cache
+#define CODAG_HD_CALL __host__ __device__ __noinline__
 #else
 #define CODAG_HD inline
+#define CODAG_HD_CALL inline
 #endif
 
 // width of 5-bit code c (__BIT_WIDTH_DECODE_MAP)
