@@ -10,8 +10,8 @@
 
 #if defined(__CUDACC__)
 #define CODAG_HD __host__ __device__ __forceinline__
-// a large step called from many places, kept as one copy so that a warp's loop fits the
-// instruction cache
+// a large step called from many places, kept out of line on the device: its registers then
+// do not add to those of every loop that calls it
 #define CODAG_HD_CALL __host__ __device__ __noinline__
 #else
 #define CODAG_HD inline
